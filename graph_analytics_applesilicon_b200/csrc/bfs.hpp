@@ -1,0 +1,99 @@
+// bfs.hpp -- the BFS handle behind gb_bfs_* (the role of gpu::GpuBfs,
+// src/metal/bfs_gpu.hpp:35-105).
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "prims.cuh"
+#include "selector.cuh"
+
+// Per-level counters of the host-driven forms (layout of the reference's
+// stats buffer, src/shaders/bfs.metal:7-21, widened to 64-bit sums).
+struct GbLevelStats {
+    unsigned found;      // vertices discovered (next frontier size / queue tail)
+    unsigned bin[3];     // gpu_binned: next-level small / medium / large queue tails
+    unsigned long long frontier;   // vertices in the input frontier
+    unsigned long long edges;      // adjacency entries examined
+    unsigned long long nextEdges;  // sum of the discovered vertices' degrees
+};
+
+// Counters of one level of the persistent kernels (triple-buffered by level).
+struct GbPCounters {
+    unsigned qtail;              // next frontier: entries in the vertex queue
+    unsigned work;               // dynamic work-item ticket of this level
+    unsigned long long hubPack;  // next frontier hubs: (count << 40) | sum of their degrees
+    unsigned long long nextEdges;// sum of degrees of everything discovered this level
+    unsigned long long examined; // adjacency entries examined (bottom-up)
+    unsigned long long found;    // vertices discovered this level
+    unsigned long long pad[2];
+};
+
+struct gb_bfs {
+    uint64_t n = 0, m = 0;
+    std::vector<uint32_t> hostRowPtr;  // degrees of sources on the host
+    gb::DevBuf<uint32_t> rowPtr, colIdx, dist;
+    gb::Stream stream;
+    gb::EventPair ev;
+    gb::ScanScratch scan;
+
+    // host-driven forms
+    gb::DevBuf<GbLevelStats> stats;
+    gb::HostPinned<GbLevelStats> hstats;
+    gb::HostPinned<uint32_t> hstage;
+    gb::DevBuf<uint32_t> qA, qB, degA, degB, bins[2][3], bmFront, bmNext;
+
+    // persistent single-source
+    gb::DevBuf<uint32_t> pq[2][3];       // queue: vertex, adjacency start, degree
+    gb::DevBuf<uint32_t> phub[2][2];     // hub list: vertex, adjacency start
+    gb::DevBuf<unsigned long long> phubOff[2];
+    gb::DevBuf<uint32_t> pbm[3];         // frontier bitmaps
+    gb::DevBuf<uint32_t> pvisited;       // visited bitmap
+    gb::DevBuf<GbPCounters> pctr;        // [3]
+    gb::DevBuf<unsigned> pctl;           // [0] barrier, [1] error, [2] levels, [3] flags
+    gb::DevBuf<gb_level> ptrace;
+    gb::DevBuf<double> pstate;           // level state for resumable (profiling) runs
+    int pGrid = 0, pBlock = 0;
+
+    // batched (64 sources)
+    gb::DevBuf<unsigned long long> bSeen, bFront[2], bNext;
+    gb::DevBuf<uint32_t> bActive[2], bCand, bHubV[2];
+    gb::DevBuf<unsigned long long> bHubOff[2];
+    gb::DevBuf<uint32_t> bDist;          // k * n results
+    int bGrid = 0, bBlock = 0;
+
+    // learned selector parameters (single-source, batched)
+    gb::DevBuf<float> selParams[2];
+    bool selLoaded[2] = {false, false};
+
+    double lastGpuMs = 0;
+    uint32_t lastLevels = 0;
+
+    uint32_t degree(uint32_t v) const { return hostRowPtr[v + 1] - hostRowPtr[v]; }
+
+    void runVertex(uint32_t src, const gb_bfs_options& o, std::vector<gb_level>* tr);
+    void runNaive(uint32_t src, const gb_bfs_options& o, std::vector<gb_level>* tr);
+    void runBinned(uint32_t src, const gb_bfs_options& o, std::vector<gb_level>* tr);
+    void runEdge(uint32_t src, const gb_bfs_options& o, std::vector<gb_level>* tr);
+    void runDirOpt(uint32_t src, const gb_bfs_options& o, std::vector<gb_level>* tr);
+    void runPersistent(uint32_t src, const gb_bfs_options& o, std::vector<gb_level>* tr);
+    void runBatch(const uint32_t* src, int k, const gb_bfs_options& o, std::vector<gb_level>* tr);
+    // Profiling (selector training data).
+    size_t profileLevels(uint32_t src, const gb_bfs_options& o, int repeats, float* feats, float* times,
+                         size_t cap);
+    size_t profileBatchLevels(const uint32_t* src, int k, const gb_bfs_options& o, int repeats,
+                              float* feats, float* times, size_t cap);
+
+    // internal helpers
+    void beginLevel();
+    void endLevel();  // copy stats, sync, accumulate GPU time
+    void initDist(uint32_t src);
+    void ensureEdgeBuffers();
+    void ensurePersistent(const gb_bfs_options& o);
+    void ensureBatch(const gb_bfs_options& o, int k);
+};
+
+namespace gb {
+uint32_t checkTg(uint32_t tg);
+void validateOptions(const gb_bfs_options& o);
+}  // namespace gb

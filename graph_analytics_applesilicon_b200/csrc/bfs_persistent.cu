@@ -1,0 +1,744 @@
+// bfs_persistent.cu -- single-source BFS with every level in one cooperative
+// launch (gpu_do_persistent; `hybrid` maps here).
+//
+// Replaces the reference's per-level command buffer + host wait
+// (src/metal/bfs_gpu.mm:83-104, ~0.1-0.2 ms per level) and the CPU half of its
+// hybrid (bfs_gpu.mm:307-325): the blocks of a co-resident grid run a level,
+// meet at a bounded grid barrier, read the level's counters from device
+// memory and all take the same next-level decision (alpha/beta rule, the
+// learned selector, or a forced strategy) without a host round trip.
+//
+// Device state (n vertices, W = ceil(n/32) words):
+//   dist u32[n]; visited bitmap u32[W]; frontier bitmaps bm[3] u32[W]
+//   (level L reads bm[L%3], writes bm[(L+1)%3], clears bm[(L+2)%3]);
+//   frontier queue q[2] = (vertex, adjacency start, degree) u32[n] each;
+//   hub list hub[2] = (vertex, start, exclusive offset in the hubs' edge space)
+//   for vertices of degree >= hub_min, whose edges are split across blocks;
+//   counters ctr[3] (level L writes ctr[L%3], zeroes ctr[(L+1)%3]).
+// Top-down claims a vertex with atomicOr on its visited bit (an L2-resident
+// word instead of a 32-bit CAS on dist); bottom-up writes only bitmaps.
+#include <algorithm>
+#include <cstring>
+
+#include "bfs.hpp"
+
+namespace gb {
+namespace {
+
+constexpr unsigned long long kHubShift = 40;
+constexpr unsigned long long kHubMask = (1ull << kHubShift) - 1;
+constexpr uint32_t kTraceCap = 1u << 16;
+
+enum { S_LEVEL, S_BOTTOMUP, S_SCOUT, S_TOCHECK, S_UNEXPLORED, S_REACHED, S_QVALID, S_LAST, S_COUNT };
+
+struct PArgs {
+    const uint32_t* __restrict__ row_ptr;
+    const uint32_t* __restrict__ col_idx;
+    uint32_t* dist;
+    uint32_t* qv[2];
+    uint32_t* qs[2];
+    uint32_t* qd[2];
+    uint32_t* hv[2];
+    uint32_t* hs[2];
+    unsigned long long* ho[2];
+    uint32_t* bm[3];
+    uint32_t* visited;
+    GbPCounters* ctr;
+    unsigned* ctl;  // [0] barrier word, [1] error flag, [2] levels run
+    gb_level* trace;
+    const float* sel;
+    double* state;
+    uint64_t n, m;
+    uint32_t words, source, hubMin, traceCap;
+    double alpha, beta;
+    int selector, force;
+    unsigned long long spinLimit;
+    uint32_t startLevel, maxLevels;
+};
+
+template <int NT>
+__device__ __forceinline__ uint32_t blockScan(uint32_t v, uint32_t* total, uint32_t* sm) {
+    constexpr int W = NT / 32;
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(kFull, x, o);
+        if ((int)lane >= o) x += y;
+    }
+    if (lane == 31) sm[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t w = lane < W ? sm[lane] : 0u, incl = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(kFull, incl, o);
+            if ((int)lane >= o) incl += y;
+        }
+        if (lane < W) sm[lane] = incl - w;
+        if (lane == W - 1) sm[W] = incl;
+    }
+    __syncthreads();
+    uint32_t r = sm[wid] + x - v;
+    *total = sm[W];
+    __syncthreads();
+    return r;
+}
+
+// Largest i in [lo, hi] with off[i] <= e.
+template <class T>
+__device__ __forceinline__ uint32_t ownerOf(const T* off, uint32_t lo, uint32_t hi, T e) {
+    while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= e) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ unsigned long long ldv(const unsigned long long* p) {
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+__device__ __forceinline__ unsigned ldv(const unsigned* p) { return *reinterpret_cast<const volatile unsigned*>(p); }
+
+// Per-thread accumulators of one level, flushed once per block.
+struct Acc {
+    unsigned long long found = 0, deg = 0, exam = 0;
+};
+
+// Claim u for level+1 (all 32 lanes call together) and append it to the next
+// frontier: bitmap bit, queue entry (degree < hub_min) or hub entry.
+__device__ __forceinline__ void discover(const PArgs& a, bool has, uint32_t u, uint32_t level, GbPCounters* cur,
+                                         uint32_t* bmNext, uint32_t nq, Acc& acc) {
+    bool claimed = false;
+    uint32_t w = u >> 5, bit = 1u << (u & 31);
+    if (has && !(a.visited[w] & bit)) claimed = !(atomicOr(&a.visited[w], bit) & bit);
+    if (!__any_sync(kFull, claimed)) return;
+    uint32_t st = 0, d = 0;
+    if (claimed) {
+        st = a.row_ptr[u];
+        d = a.row_ptr[u + 1] - st;
+        a.dist[u] = level + 1;
+        atomicOr(&bmNext[w], bit);
+        acc.found++;
+        acc.deg += d;
+    }
+    const bool hub = claimed && d >= a.hubMin;
+    const bool q = claimed && !hub;
+    if (__any_sync(kFull, q)) {
+        uint32_t pos = warpAppend(q, &cur->qtail);
+        if (q) {
+            a.qv[nq][pos] = u;
+            a.qs[nq][pos] = st;
+            a.qd[nq][pos] = d;
+        }
+    }
+    if (hub) {
+        unsigned long long old = atomicAdd(&cur->hubPack, (1ull << kHubShift) | d);
+        uint32_t i = (uint32_t)(old >> kHubShift);
+        a.hv[nq][i] = u;
+        a.hs[nq][i] = st;
+        a.ho[nq][i] = old & kHubMask;
+    }
+}
+
+template <int NT>
+struct Smem {
+    uint32_t scan[NT / 32 + 1];
+    uint32_t off[NT];
+    uint32_t st[NT];
+    float sel[kSelParams];
+    unsigned long long acc[3];
+    uint32_t range[2];
+    unsigned item;
+    int strat;
+    uint32_t base;
+};
+
+// Edge-balanced expansion of one tile of NT queue entries: the entries'
+// degrees are scanned in shared memory and every thread takes EPT edges per
+// round (thread t: edges base + k*NT + t), owner found by a shared-memory
+// binary search over the staged offsets.
+template <int NT, int EPT>
+__device__ void tdTile(const PArgs& a, Smem<NT>& sm, uint32_t item, uint32_t S, uint32_t qc, uint32_t level,
+                       GbPCounters* cur, uint32_t* bmNext, Acc& acc) {
+    const uint32_t idx = item * NT + threadIdx.x;
+    uint32_t st = 0, d = 0;
+    if (idx < S) {
+        st = a.qs[qc][idx];
+        d = a.qd[qc][idx];
+    }
+    uint32_t tot;
+    const uint32_t off = blockScan<NT>(d, &tot, sm.scan);
+    sm.off[threadIdx.x] = off;
+    sm.st[threadIdx.x] = st;
+    __syncthreads();
+    const uint32_t cnt = min((uint32_t)NT, S - item * NT);
+    for (uint32_t base = 0; base < tot; base += NT * EPT) {
+        uint32_t u[EPT];
+        bool has[EPT];
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const uint32_t e = base + k * NT + threadIdx.x;
+            has[k] = e < tot;
+            u[k] = 0;
+            if (has[k]) {
+                const uint32_t o = ownerOf(sm.off, 0u, cnt - 1, e);
+                u[k] = a.col_idx[sm.st[o] + (e - sm.off[o])];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) discover(a, has[k], u[k], level, cur, bmNext, qc ^ 1u, acc);
+    }
+    __syncthreads();
+}
+
+// Warp per queue entry (degree-binned form): lanes stride the adjacency list.
+template <int NT>
+__device__ void tdWarpItem(const PArgs& a, uint32_t item, uint32_t S, uint32_t qc, uint32_t level, GbPCounters* cur,
+                           uint32_t* bmNext, Acc& acc) {
+    const uint32_t idx = item * (NT / 32) + (threadIdx.x >> 5);
+    if (idx >= S) return;  // warp-uniform
+    const uint32_t st = a.qs[qc][idx], d = a.qd[qc][idx];
+    for (uint32_t base = 0; base < d; base += 32) {
+        const uint32_t e = base + laneId();
+        const bool has = e < d;
+        discover(a, has, has ? a.col_idx[st + e] : 0u, level, cur, bmNext, qc ^ 1u, acc);
+    }
+}
+
+// One chunk of the hubs' concatenated edge space, split over the block.
+template <int NT>
+__device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e1, uint32_t H, uint32_t qc,
+                           uint32_t level, GbPCounters* cur, uint32_t* bmNext, Acc& acc) {
+    const unsigned long long* ho = a.ho[qc];
+    if (threadIdx.x == 0) {
+        uint32_t lo = ownerOf(ho, 0u, H - 1, (unsigned long long)e0);
+        sm.range[0] = lo;
+        sm.range[1] = ownerOf(ho, lo, H - 1, (unsigned long long)(e1 - 1));
+    }
+    __syncthreads();
+    const uint32_t lo = sm.range[0], hi = sm.range[1];
+    for (uint64_t base = e0; base < e1; base += NT) {
+        const uint64_t e = base + threadIdx.x;
+        const bool has = e < e1;
+        uint32_t u = 0;
+        if (has) {
+            const uint32_t o = ownerOf(ho, lo, hi, (unsigned long long)e);
+            u = a.col_idx[a.hs[qc][o] + (uint32_t)(e - ho[o])];
+        }
+        discover(a, has, u, level, cur, bmNext, qc ^ 1u, acc);
+    }
+    __syncthreads();
+}
+
+// Bottom-up: warp per visited-bitmap word; each unvisited lane scans its list
+// for the first neighbour in the frontier bitmap (early exit).  The found
+// lanes form the next frontier word (__ballot_sync); the owning warp writes
+// it and the visited word with plain stores.
+__device__ void buLevel(const PArgs& a, uint32_t level, Acc& acc) {
+    const uint32_t* front = a.bm[level % 3];
+    uint32_t* next = a.bm[(level + 1) % 3];
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const unsigned lane = laneId();
+    for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.words; w += nwarps) {
+        const uint32_t vw = a.visited[w];
+        if (vw == kFull) continue;  // warp-uniform
+        const uint32_t v = (uint32_t)(w * 32 + lane);
+        bool found = false;
+        uint32_t b = 0, e = 0;
+        if (!((vw >> lane) & 1u)) {
+            b = a.row_ptr[v];
+            e = a.row_ptr[v + 1];
+            uint32_t i = b;
+            for (; i < e; ++i) {
+                const uint32_t u = a.col_idx[i];
+                if ((front[u >> 5] >> (u & 31)) & 1u) {
+                    found = true;
+                    ++i;
+                    break;
+                }
+            }
+            acc.exam += i - b;
+        }
+        const unsigned F = __ballot_sync(kFull, found);
+        if (found) {
+            a.dist[v] = level + 1;
+            acc.deg += e - b;
+            acc.found++;
+        }
+        if (lane == 0 && F) {
+            next[w] = F;
+            a.visited[w] = vw | F;
+        }
+    }
+}
+
+// Frontier bitmap -> queue + hub list (only after a bottom-up level, when the
+// next level runs top-down).  Per block-round of NT words: per-thread counts,
+// a block scan, one atomic for the block's queue range.
+template <int NT>
+__device__ void bitmapToQueue(const PArgs& a, Smem<NT>& sm, uint32_t level, GbPCounters* prev) {
+    const uint32_t* bm = a.bm[level % 3];
+    const uint32_t qc = level & 1u;
+    for (uint64_t t0 = (uint64_t)blockIdx.x * NT; t0 < a.words; t0 += (uint64_t)gridDim.x * NT) {
+        const uint64_t w = t0 + threadIdx.x;
+        const uint32_t word = w < a.words ? bm[w] : 0u;
+        uint32_t c = 0;
+        for (uint32_t x = word; x; x &= x - 1) {
+            const uint32_t v = (uint32_t)(w * 32 + __ffs(x) - 1);
+            const uint32_t st = a.row_ptr[v], d = a.row_ptr[v + 1] - st;
+            if (d >= a.hubMin) {
+                unsigned long long old = atomicAdd(&prev->hubPack, (1ull << kHubShift) | d);
+                uint32_t i = (uint32_t)(old >> kHubShift);
+                a.hv[qc][i] = v;
+                a.hs[qc][i] = st;
+                a.ho[qc][i] = old & kHubMask;
+            } else {
+                ++c;
+            }
+        }
+        uint32_t tot;
+        uint32_t pos = blockScan<NT>(c, &tot, sm.scan);
+        if (threadIdx.x == 0) sm.base = tot ? atomicAdd(&prev->qtail, tot) : 0u;
+        __syncthreads();
+        pos += sm.base;
+        for (uint32_t x = word; x; x &= x - 1) {
+            const uint32_t v = (uint32_t)(w * 32 + __ffs(x) - 1);
+            const uint32_t st = a.row_ptr[v], d = a.row_ptr[v + 1] - st;
+            if (d < a.hubMin) {
+                a.qv[qc][pos] = v;
+                a.qs[qc][pos] = st;
+                a.qd[qc][pos] = d;
+                ++pos;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
+    __shared__ Smem<NT> sm;
+    const unsigned tid = threadIdx.x;
+    const uint64_t gtid = (uint64_t)blockIdx.x * NT + tid, gthreads = (uint64_t)gridDim.x * NT;
+    unsigned* bar = &a.ctl[0];
+    unsigned* err = &a.ctl[1];
+    const bool learned = a.selector == GB_SELECT_LEARNED && a.sel != nullptr;
+    if (learned)
+        for (int i = tid; i < kSelParams; i += NT) sm.sel[i] = a.sel[i];
+
+    uint32_t level;
+    bool bottomUp, qValid;
+    uint64_t scout, toCheck, unexplored, reached;
+    int lastStrat;
+    if (a.startLevel == 0) {
+        uint4* d4 = reinterpret_cast<uint4*>(a.dist);
+        for (uint64_t i = gtid; i < a.n / 4; i += gthreads) d4[i] = make_uint4(kInf, kInf, kInf, kInf);
+        for (uint64_t i = a.n / 4 * 4 + gtid; i < a.n; i += gthreads) a.dist[i] = kInf;
+        for (uint64_t w = gtid; w < a.words; w += gthreads) {
+            uint32_t pad = 0;
+            if (w == a.words - 1 && (a.n & 31)) pad = ~((1u << (a.n & 31)) - 1u);  // bits past n read as visited
+            a.visited[w] = pad;
+            a.bm[0][w] = 0;
+            a.bm[1][w] = 0;
+            a.bm[2][w] = 0;
+        }
+        if (gtid == 0)
+            for (int s = 0; s < 3; ++s) a.ctr[s] = GbPCounters{};
+        if (!gridBarrier(bar, err, a.spinLimit)) return;
+        const uint32_t src = a.source;
+        const uint32_t st = a.row_ptr[src], d = a.row_ptr[src + 1] - st;
+        if (gtid == 0) {
+            a.dist[src] = 0;
+            a.visited[src >> 5] |= 1u << (src & 31);
+            a.bm[0][src >> 5] |= 1u << (src & 31);
+            GbPCounters& c = a.ctr[2];
+            c.found = 1;
+            c.nextEdges = d;
+            if (d >= a.hubMin) {
+                a.hv[0][0] = src;
+                a.hs[0][0] = st;
+                a.ho[0][0] = 0;
+                c.hubPack = (1ull << kHubShift) | d;
+            } else {
+                a.qv[0][0] = src;
+                a.qs[0][0] = st;
+                a.qd[0][0] = d;
+                c.qtail = 1;
+            }
+        }
+        if (!gridBarrier(bar, err, a.spinLimit)) return;
+        level = 0;
+        bottomUp = false;
+        qValid = true;
+        scout = d;
+        toCheck = a.m;
+        unexplored = a.m - d;
+        reached = 1;
+        lastStrat = -1;
+    } else {
+        level = (uint32_t)a.state[S_LEVEL];
+        bottomUp = a.state[S_BOTTOMUP] != 0;
+        scout = (uint64_t)a.state[S_SCOUT];
+        toCheck = (uint64_t)a.state[S_TOCHECK];
+        unexplored = (uint64_t)a.state[S_UNEXPLORED];
+        reached = (uint64_t)a.state[S_REACHED];
+        qValid = a.state[S_QVALID] != 0;
+        lastStrat = (int)a.state[S_LAST];
+        if (!gridBarrier(bar, err, a.spinLimit)) return;
+    }
+    const uint32_t endLevel = a.maxLevels ? a.startLevel + a.maxLevels : 0xFFFFFFFFu;
+    uint64_t tPrev = globaltimer();
+
+    for (;;) {
+        GbPCounters* prev = &a.ctr[(level + 2) % 3];
+        GbPCounters* cur = &a.ctr[level % 3];
+        const uint64_t size = ldv(&prev->found), fedges = ldv(&prev->nextEdges);
+        if (size == 0 || level >= endLevel) break;
+
+        // alpha/beta rule (src/cpu/bfs_cpu.cpp:247-279): always evaluated, it
+        // is the fallback and the judge of the learned choice.
+        if (!bottomUp && (double)scout > (double)toCheck / a.alpha) bottomUp = true;
+        if (!bottomUp) toCheck -= min(toCheck, scout);
+        const int ruleStrat = bottomUp ? GB_STRAT_BU : GB_STRAT_TD_EPT2;
+        int strat = ruleStrat;
+        if (a.force >= 0) {
+            strat = a.force;
+        } else if (learned) {
+            if (tid < 32) {
+                float f[kSelFeatures];
+                selectorFeatures((double)size, (double)fedges, (double)unexplored, (double)(a.n - reached),
+                                 (double)a.n, (double)a.m, (double)level, f);
+                int s = selectorArgmin(sm.sel, f, tid);
+                if (tid == 0) sm.strat = s;
+            }
+            __syncthreads();
+            if (sm.strat >= 0) strat = sm.strat;
+        }
+        if (tid == 0) {
+            sm.acc[0] = sm.acc[1] = sm.acc[2] = 0;
+        }
+        if (gtid == 0) {
+            if (a.trace && level > 0 && level - 1 < a.traceCap && lastStrat == GB_STRAT_BU)
+                a.trace[level - 1].edges = ldv(&prev->examined);
+            if (a.trace && level < a.traceCap) {
+                gb_level r;
+                r.level = level;
+                r.direction = strat == GB_STRAT_BU ? 'B' : 'T';
+                r.device = 'G';
+                r.strategy = (uint8_t)strat;
+                r.pad = (uint8_t)ruleStrat;
+                r.frontier = size;
+                r.edges = fedges;
+                r.time_ms = 0;
+                a.trace[level] = r;
+            }
+            a.ctr[(level + 1) % 3] = GbPCounters{};
+        }
+        uint32_t* clearBm = a.bm[(level + 2) % 3];
+        for (uint64_t w = gtid; w < a.words; w += gthreads) clearBm[w] = 0;
+        __syncthreads();
+
+        Acc acc;
+        if (strat == GB_STRAT_BU) {
+            buLevel(a, level, acc);
+        } else {
+            if (!qValid) {
+                bitmapToQueue<NT>(a, sm, level, prev);
+                if (!gridBarrier(bar, err, a.spinLimit)) return;
+            }
+            const uint32_t qc = level & 1u;
+            const uint32_t S = ldv(&prev->qtail);
+            const unsigned long long hp = ldv(&prev->hubPack);
+            const uint32_t H = (uint32_t)(hp >> kHubShift);
+            const uint64_t HE = hp & kHubMask;
+            const uint32_t per = strat == GB_STRAT_TD_WARP ? NT / 32 : NT;
+            const uint32_t nt = (S + per - 1) / per;
+            const uint64_t HC = (uint64_t)NT * 8;
+            const uint32_t nh = (uint32_t)((HE + HC - 1) / HC);
+            uint32_t* bmNext = a.bm[(level + 1) % 3];
+            for (;;) {
+                if (tid == 0) sm.item = atomicAdd(&cur->work, 1u);
+                __syncthreads();
+                const uint32_t item = sm.item;
+                __syncthreads();
+                if (item >= nt + nh) break;
+                if (item < nt) {
+                    switch (strat) {
+                        case GB_STRAT_TD_EPT1: tdTile<NT, 1>(a, sm, item, S, qc, level, cur, bmNext, acc); break;
+                        case GB_STRAT_TD_EPT4: tdTile<NT, 4>(a, sm, item, S, qc, level, cur, bmNext, acc); break;
+                        case GB_STRAT_TD_WARP: tdWarpItem<NT>(a, item, S, qc, level, cur, bmNext, acc); break;
+                        default: tdTile<NT, 2>(a, sm, item, S, qc, level, cur, bmNext, acc); break;
+                    }
+                } else {
+                    const uint64_t e0 = (uint64_t)(item - nt) * HC;
+                    tdHubChunk<NT>(a, sm, e0, min(e0 + HC, HE), H, qc, level, cur, bmNext, acc);
+                }
+            }
+        }
+        // one atomic per block and counter
+        unsigned long long f = warpSum(acc.found), dg = warpSum(acc.deg), ex = warpSum(acc.exam);
+        if (laneId() == 0) {
+            if (f) atomicAdd(&sm.acc[0], f);
+            if (dg) atomicAdd(&sm.acc[1], dg);
+            if (ex) atomicAdd(&sm.acc[2], ex);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            if (sm.acc[0]) atomicAdd(&cur->found, sm.acc[0]);
+            if (sm.acc[1]) atomicAdd(&cur->nextEdges, sm.acc[1]);
+            if (sm.acc[2]) atomicAdd(&cur->examined, sm.acc[2]);
+        }
+        if (!gridBarrier(bar, err, a.spinLimit)) return;
+        if (gtid == 0) {
+            const uint64_t t = globaltimer();
+            if (a.trace && level < a.traceCap) a.trace[level].time_ms = (double)(t - tPrev) * 1e-6;
+            tPrev = t;
+        }
+        const uint64_t found = ldv(&cur->found), nextE = ldv(&cur->nextEdges);
+        reached += found;
+        unexplored -= min(unexplored, nextE);
+        if (bottomUp) {
+            if (!(found >= size || (double)found > (double)a.n / a.beta)) {
+                bottomUp = false;
+                scout = 1;
+            }
+        } else {
+            scout = nextE;
+        }
+        qValid = strat != GB_STRAT_BU;
+        lastStrat = strat;
+        ++level;
+    }
+    if (gtid == 0) {
+        if (a.trace && level > 0 && level - 1 < a.traceCap && lastStrat == GB_STRAT_BU)
+            a.trace[level - 1].edges = ldv(&a.ctr[(level + 2) % 3].examined);
+        a.ctl[2] = level;
+        a.state[S_LEVEL] = level;
+        a.state[S_BOTTOMUP] = bottomUp;
+        a.state[S_SCOUT] = (double)scout;
+        a.state[S_TOCHECK] = (double)toCheck;
+        a.state[S_UNEXPLORED] = (double)unexplored;
+        a.state[S_REACHED] = (double)reached;
+        a.state[S_QVALID] = qValid;
+        a.state[S_LAST] = lastStrat;
+    }
+}
+
+template <int NT>
+void launchPersistent(gb_bfs& h, PArgs& a) {
+    void* args[] = {&a};
+    GB_CUDA(cudaLaunchCooperativeKernel((void*)persistentBfsKernel<NT>, dim3(h.pGrid), dim3(NT), args, 0, h.stream.s));
+}
+
+PArgs makeArgs(gb_bfs& h, const gb_bfs_options& o, uint32_t src) {
+    PArgs a{};
+    a.row_ptr = h.rowPtr.get();
+    a.col_idx = h.colIdx.get();
+    a.dist = h.dist.get();
+    for (int i = 0; i < 2; ++i) {
+        a.qv[i] = h.pq[i][0].get();
+        a.qs[i] = h.pq[i][1].get();
+        a.qd[i] = h.pq[i][2].get();
+        a.hv[i] = h.phub[i][0].get();
+        a.hs[i] = h.phub[i][1].get();
+        a.ho[i] = h.phubOff[i].get();
+    }
+    for (int i = 0; i < 3; ++i) a.bm[i] = h.pbm[i].get();
+    a.visited = h.pvisited.get();
+    a.ctr = h.pctr.get();
+    a.ctl = h.pctl.get();
+    a.trace = h.ptrace.get();
+    a.traceCap = kTraceCap;
+    a.sel = h.selLoaded[0] ? h.selParams[0].get() : nullptr;
+    a.state = h.pstate.get();
+    a.n = h.n;
+    a.m = h.m;
+    a.words = (uint32_t)((h.n + 31) / 32);
+    a.source = src;
+    a.hubMin = std::max<uint32_t>(o.hub_min, 32);
+    a.alpha = o.alpha;
+    a.beta = o.beta;
+    a.selector = (int)o.selector;
+    a.force = o.force_strategy;
+    a.spinLimit = o.spin_limit ? o.spin_limit : (1ull << 24);
+    a.startLevel = 0;
+    a.maxLevels = 0;
+    return a;
+}
+
+void launchFor(gb_bfs& h, PArgs& a) {
+    if (h.pBlock == 256) launchPersistent<256>(h, a);
+    else launchPersistent<512>(h, a);
+}
+
+}  // namespace
+}  // namespace gb
+
+using namespace gb;
+
+void gb_bfs::ensurePersistent(const gb_bfs_options& o) {
+    const int block = o.block ? (int)o.block : 512;
+    const uint64_t hubCap = std::min<uint64_t>(n, m / 32 + 1);
+    for (int i = 0; i < 2; ++i) {
+        for (int j = 0; j < 3; ++j) pq[i][j].ensure(n);
+        for (int j = 0; j < 2; ++j) phub[i][j].ensure(hubCap);
+        phubOff[i].ensure(hubCap);
+    }
+    const uint64_t words = (n + 31) / 32;
+    for (auto& b : pbm) b.ensure(words);
+    pvisited.ensure(words);
+    pctr.ensure(3);
+    pctl.ensure(4);
+    ptrace.ensure(kTraceCap);
+    pstate.ensure(S_COUNT);
+    if (pBlock != block) {
+        int perSm = 0;
+        if (block == 256)
+            GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, persistentBfsKernel<256>, 256, 0));
+        else
+            GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, persistentBfsKernel<512>, 512, 0));
+        if (perSm < 1) throw Error(GB_ERR_CUDA, "persistent BFS kernel cannot be resident");
+        pGrid = perSm * deviceSmCount();
+        pBlock = block;
+    }
+}
+
+void gb_bfs::runPersistent(uint32_t src, const gb_bfs_options& o, std::vector<gb_level>* tr) {
+    validateOptions(o);
+    ensurePersistent(o);
+    PArgs a = makeArgs(*this, o, src);
+    if (o.selector == GB_SELECT_LEARNED && !selLoaded[0])
+        throw Error(GB_ERR_STATE, "learned selector requested but no parameters are loaded");
+    GB_CUDA(cudaMemsetAsync(pctl.get(), 0, 4 * sizeof(unsigned), stream.s));
+    GB_CUDA(cudaEventRecord(ev.a, stream.s));
+    launchFor(*this, a);
+    GB_CUDA(cudaEventRecord(ev.b, stream.s));
+    unsigned ctl[4];
+    GB_CUDA(cudaMemcpyAsync(ctl, pctl.get(), sizeof ctl, cudaMemcpyDeviceToHost, stream.s));
+    GB_CUDA(cudaStreamSynchronize(stream.s));
+    lastGpuMs = ev.ms();
+    lastLevels = ctl[2];
+    if (ctl[1]) throw Error(GB_ERR_TIMEOUT, "persistent BFS: grid barrier wait exceeded its spin limit");
+    if (tr) {
+        const uint32_t k = std::min<uint32_t>(ctl[2], kTraceCap);
+        std::vector<gb_level> t(k);
+        if (k) GB_CUDA(cudaMemcpy(t.data(), ptrace.get(), k * sizeof(gb_level), cudaMemcpyDeviceToHost));
+        for (auto& r : t) r.pad = 0;
+        tr->insert(tr->end(), t.begin(), t.end());
+    }
+}
+
+// Selector training data: advance the BFS one level at a time (alpha/beta
+// rule), and before each level time every strategy from the same state
+// (device buffers snapshotted and restored), each a one-level cooperative
+// launch timed inside the kernel between two grid barriers.
+size_t gb_bfs::profileLevels(uint32_t src, const gb_bfs_options& o0, int repeats, float* feats, float* times,
+                             size_t cap) {
+    gb_bfs_options o = o0;
+    o.selector = GB_SELECT_RULE;
+    validateOptions(o);
+    ensurePersistent(o);
+    const uint64_t words = (n + 31) / 32;
+    // snapshot buffers
+    DevBuf<uint32_t> sDist, sQ[3], sHub[2], sBm[3], sVis;
+    DevBuf<unsigned long long> sHo;
+    DevBuf<GbPCounters> sCtr;
+    DevBuf<double> sState;
+    sDist.ensure(n);
+    for (auto& b : sQ) b.ensure(n);
+    const uint64_t hubCap = std::min<uint64_t>(n, m / 32 + 1);
+    for (auto& b : sHub) b.ensure(hubCap);
+    sHo.ensure(hubCap);
+    for (auto& b : sBm) b.ensure(words);
+    sVis.ensure(words);
+    sCtr.ensure(3);
+    sState.ensure(S_COUNT);
+    auto copy = [&](void* dst, const void* srcp, size_t bytes) {
+        GB_CUDA(cudaMemcpyAsync(dst, srcp, bytes, cudaMemcpyDeviceToDevice, stream.s));
+    };
+    int qc = 0;
+    auto snapshot = [&](bool save) {
+        auto mv = [&](void* a, void* b, size_t bytes) { save ? copy(a, b, bytes) : copy(b, a, bytes); };
+        mv(sDist.get(), dist.get(), n * 4);
+        for (int j = 0; j < 3; ++j) mv(sQ[j].get(), pq[qc][j].get(), n * 4);
+        for (int j = 0; j < 2; ++j) mv(sHub[j].get(), phub[qc][j].get(), hubCap * 4);
+        mv(sHo.get(), phubOff[qc].get(), hubCap * 8);
+        for (int j = 0; j < 3; ++j) mv(sBm[j].get(), pbm[j].get(), words * 4);
+        mv(sVis.get(), pvisited.get(), words * 4);
+        mv(sCtr.get(), pctr.get(), 3 * sizeof(GbPCounters));
+        mv(sState.get(), pstate.get(), S_COUNT * sizeof(double));
+    };
+    auto run = [&](uint32_t startLevel, uint32_t maxLevels, int force) {
+        PArgs a = makeArgs(*this, o, src);
+        a.startLevel = startLevel;
+        a.maxLevels = maxLevels;
+        a.force = force;
+        a.selector = GB_SELECT_RULE;
+        GB_CUDA(cudaMemsetAsync(pctl.get(), 0, 4 * sizeof(unsigned), stream.s));
+        launchFor(*this, a);
+        unsigned ctl[4];
+        GB_CUDA(cudaMemcpyAsync(ctl, pctl.get(), sizeof ctl, cudaMemcpyDeviceToHost, stream.s));
+        GB_CUDA(cudaStreamSynchronize(stream.s));
+        if (ctl[1]) throw Error(GB_ERR_TIMEOUT, "profiling run: grid barrier timeout");
+        return ctl[2];
+    };
+    // Level 0 has no saved state to restore: each strategy is timed by a
+    // fresh launch (prologue + level 0); later levels restore the snapshot.
+    size_t rows = 0;
+    std::vector<double> st(S_COUNT);
+    std::vector<GbPCounters> ctr(3);
+    for (uint32_t level = 0;; ++level) {
+        if (level == 0) {
+            // Prologue + level 0 with each strategy, from scratch every time.
+            float best[GB_NUM_STRATS];
+            for (int k = 0; k < GB_NUM_STRATS; ++k) {
+                best[k] = 1e30f;
+                for (int r = 0; r < repeats; ++r) {
+                    run(0, 1, k);
+                    gb_level t;
+                    GB_CUDA(cudaMemcpy(&t, ptrace.get(), sizeof t, cudaMemcpyDeviceToHost));
+                    best[k] = std::min(best[k], (float)(t.time_ms * 1e3));
+                }
+            }
+            const uint32_t d0 = degree(src);
+            if (rows < cap) {
+                selectorFeatures(1.0, (double)d0, (double)(m - d0), (double)(n - 1), (double)n, (double)m, 0.0,
+                                 feats + rows * kSelFeatures);
+                for (int k = 0; k < GB_NUM_STRATS; ++k) times[rows * GB_NUM_STRATS + k] = best[k];
+            }
+            ++rows;
+            run(0, 1, -1);  // advance with the rule
+            qc = 1;
+            continue;
+        }
+        GB_CUDA(cudaMemcpy(st.data(), pstate.get(), S_COUNT * sizeof(double), cudaMemcpyDeviceToHost));
+        GB_CUDA(cudaMemcpy(ctr.data(), pctr.get(), 3 * sizeof(GbPCounters), cudaMemcpyDeviceToHost));
+        const GbPCounters& prev = ctr[(level + 2) % 3];
+        if (prev.found == 0) break;
+        qc = (int)(level & 1);
+        snapshot(true);
+        float best[GB_NUM_STRATS];
+        for (int k = 0; k < GB_NUM_STRATS; ++k) {
+            best[k] = 1e30f;
+            for (int r = 0; r < repeats; ++r) {
+                snapshot(false);
+                run(level, 1, k);
+                gb_level t;
+                GB_CUDA(cudaMemcpy(&t, ptrace.get() + std::min<uint32_t>(level, kTraceCap - 1), sizeof t,
+                                   cudaMemcpyDeviceToHost));
+                best[k] = std::min(best[k], (float)(t.time_ms * 1e3));
+            }
+        }
+        if (rows < cap) {
+            selectorFeatures((double)prev.found, (double)prev.nextEdges, st[S_UNEXPLORED], (double)n - st[S_REACHED],
+                             (double)n, (double)m, (double)level, feats + rows * kSelFeatures);
+            for (int k = 0; k < GB_NUM_STRATS; ++k) times[rows * GB_NUM_STRATS + k] = best[k];
+        }
+        ++rows;
+        snapshot(false);
+        run(level, 1, -1);
+    }
+    return std::min(rows, cap);
+}

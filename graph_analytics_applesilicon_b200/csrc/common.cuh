@@ -1,0 +1,198 @@
+// common.cuh -- shared host/device helpers of the B200 graph library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "graph_b200.h"
+
+namespace gb {
+
+constexpr uint32_t kInf = 0xFFFFFFFFu;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// Errors thrown inside the library and turned into gb_status at the C ABI.
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+inline void cudaCheck(cudaError_t e, const char* what, const char* file, int line) {
+    if (e != cudaSuccess) {
+        int st = (e == cudaErrorMemoryAllocation) ? GB_ERR_OOM : GB_ERR_CUDA;
+        throw Error(st, std::string(what) + " failed at " + file + ":" + std::to_string(line) + ": " +
+                            cudaGetErrorString(e));
+    }
+}
+#define GB_CUDA(x) ::gb::cudaCheck((x), #x, __FILE__, __LINE__)
+#define GB_LAUNCH_CHECK() ::gb::cudaCheck(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+#define GB_REQUIRE(cond, msg)                                   \
+    do {                                                        \
+        if (!(cond)) throw ::gb::Error(GB_ERR_ARG, (msg));      \
+    } while (0)
+
+// Owning device allocation (cudaMalloc'd, freed on destruction).
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    // (Re)allocate for at least `count` elements; contents are not kept.
+    void ensure(size_t count) {
+        if (count <= n && p) return;
+        release();
+        size_t bytes = (count ? count : 1) * sizeof(T);
+        bytes = (bytes + 255) & ~size_t(255);
+        GB_CUDA(cudaMalloc(&p, bytes));
+        n = bytes / sizeof(T);
+    }
+    T* get() const { return p; }
+};
+
+// Pinned host allocation.
+template <class T>
+struct HostPinned {
+    T* p = nullptr;
+    size_t n = 0;
+    ~HostPinned() {
+        if (p) cudaFreeHost(p);
+    }
+    void ensure(size_t count) {
+        if (count <= n && p) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        GB_CUDA(cudaMallocHost(&p, (count ? count : 1) * sizeof(T)));
+        n = count;
+    }
+};
+
+struct Stream {
+    cudaStream_t s = nullptr;
+    Stream() { GB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    ~Stream() {
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    EventPair() {
+        GB_CUDA(cudaEventCreate(&a));
+        GB_CUDA(cudaEventCreate(&b));
+    }
+    ~EventPair() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+    float ms() const {
+        float t = 0;
+        GB_CUDA(cudaEventElapsedTime(&t, a, b));
+        return t;
+    }
+};
+
+inline int deviceSmCount() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        GB_CUDA(cudaGetDevice(&dev));
+        GB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return sms;
+}
+
+inline uint32_t divUp(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+// ------------------------------------------------------------ device helpers
+
+#ifdef __CUDACC__
+__device__ __forceinline__ unsigned laneId() { return threadIdx.x & 31u; }
+__device__ __forceinline__ unsigned lanemaskLt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+template <class T>
+__device__ __forceinline__ T warpSum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ldAcquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned ldVolatile(const unsigned* p) {
+    return *reinterpret_cast<const volatile unsigned*>(p);
+}
+
+// Warp-aggregated append: every lane of the warp calls it (uniform control
+// flow); lanes with want=true get consecutive slots from *counter.
+__device__ __forceinline__ unsigned warpAppend(bool want, unsigned* counter) {
+    unsigned ballot = __ballot_sync(kFull, want);
+    unsigned base = 0;
+    if (ballot) {
+        int leader = __ffs(ballot) - 1;
+        if ((int)laneId() == leader) base = atomicAdd(counter, (unsigned)__popc(ballot));
+        base = __shfl_sync(kFull, base, leader);
+    }
+    return base + __popc(ballot & lanemaskLt());
+}
+
+// Grid-wide barrier for a co-resident (cooperative) grid.  A single counter:
+// block 0 adds 0x80000000 - (nblocks - 1), the others add 1, so the top bit
+// flips exactly when the last block arrives.  The wait is bounded: after
+// spin_limit polls (or once another block has flagged an error) the block
+// records GB timeout in *err and returns false; callers then leave the kernel.
+__device__ __forceinline__ bool gridBarrierN(unsigned* bar, unsigned* err, unsigned long long spinLimit,
+                                             unsigned nblocks) {
+    __shared__ int sOk;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned inc = (blockIdx.x == 0) ? (0x80000000u - (nblocks - 1)) : 1u;
+        __threadfence();
+        unsigned old = atomicAdd(bar, inc);
+        unsigned long long polls = 0;
+        int ok = 1;
+        while (((old ^ ldAcquire(bar)) & 0x80000000u) == 0) {
+            if (++polls > spinLimit || ldVolatile(err) != 0) {
+                atomicOr(err, 1u);
+                ok = 0;
+                break;
+            }
+            if (polls > 64) __nanosleep(64);
+        }
+        __threadfence();
+        sOk = ok && ldVolatile(err) == 0;
+    }
+    __syncthreads();
+    return sOk != 0;
+}
+
+__device__ __forceinline__ bool gridBarrier(unsigned* bar, unsigned* err, unsigned long long spinLimit) {
+    return gridBarrierN(bar, err, spinLimit, gridDim.x);
+}
+#endif
+
+}  // namespace gb

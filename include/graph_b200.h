@@ -1,0 +1,272 @@
+/*
+ * graph_b200.h -- C ABI of the B200 (sm_100a) BFS / PageRank library.
+ *
+ * This is the drop-in boundary for graph-gpu's GPU hot paths.  Each entry point
+ * names the reference interface it replaces (paths inside the reference
+ * project).  Plain pointers and sizes only; no exceptions cross the ABI:
+ * every function returns a gb_status and gb_last_error() holds the message of
+ * the calling thread's last failure.
+ *
+ * Threading: a handle owns one CUDA stream and its device buffers; it is not
+ * thread-safe (as the reference's single encoder, src/metal/primitives.hpp:1-12).
+ * All work is asynchronous on that stream and synchronised before return.
+ * Graphs: CSR with uint32 offsets/ids (src/graph/csr.hpp:29-45), m < 2^32.
+ */
+#ifndef GRAPH_B200_H
+#define GRAPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GB_UNREACHED 0xFFFFFFFFu /* cpu::kUnreached, src/cpu/bfs_cpu.hpp:14 */
+
+typedef enum {
+    GB_OK = 0,
+    GB_ERR_ARG = 1,         /* invalid argument: std::runtime_error in the reference */
+    GB_ERR_CUDA = 2,        /* CUDA runtime / kernel failure (reference: exit(1)) */
+    GB_ERR_OOM = 3,         /* device allocation failed */
+    GB_ERR_TIMEOUT = 4,     /* a bounded device wait (grid barrier) gave up */
+    GB_ERR_STATE = 5,       /* call out of order (e.g. ranks before run) */
+    GB_ERR_IO = 6,          /* .bin read/write failure */
+    GB_ERR_CAPACITY = 7     /* output buffer too small */
+} gb_status;
+
+const char* gb_last_error(void);
+/* Library version and the device it will use (name, SM count). */
+int gb_device_info(char* name, size_t cap, int* sm_count, int* cc_major, int* cc_minor);
+
+/* ------------------------------------------------------------ host graphs */
+
+#define GB_FLAG_DIRECTED 1u /* graph::kFlagDirected, src/graph/csr.hpp:14-18 */
+#define GB_FLAG_SORTED 2u
+#define GB_FLAG_DEDUP 4u
+
+/* A host CSR whose arrays the library allocated; release with gb_csr_free. */
+typedef struct {
+    uint64_t n, m;
+    uint32_t flags;
+    uint32_t* row_ptr; /* n + 1 */
+    uint32_t* col_idx; /* m */
+} gb_csr;
+
+void gb_csr_free(gb_csr* g);
+/* graph::load / graph::save, "GGPUCSR1" format (src/graph/csr.cpp:30-84). */
+int gb_csr_load(const char* path, gb_csr* out);
+int gb_csr_save(const gb_csr* g, const char* path);
+/* graph::validate (src/graph/csr.cpp:86-104); msg gets "" when valid. */
+int gb_csr_validate(const gb_csr* g, char* msg, size_t cap);
+/* graph::fromEdgeList (src/graph/csr.cpp:146-163). */
+int gb_csr_from_edges(uint64_t n, const uint32_t* eu, const uint32_t* ev, uint64_t ne, int directed,
+                      gb_csr* out);
+/* graph::transpose / symmetrize / permute (src/graph/transform.cpp:9-76). */
+int gb_csr_transpose(const gb_csr* g, gb_csr* out);
+int gb_csr_symmetrize(const gb_csr* g, gb_csr* out);
+int gb_csr_permute(const gb_csr* g, const uint32_t* perm, gb_csr* out);
+/* reorder::compute(..., "random", seed) (src/graph/reorder.cpp:20-25). */
+int gb_random_perm(uint64_t n, uint64_t seed, uint32_t* perm);
+
+/* Generators: src/graph/generators.cpp:8-75 (same graphs, byte for byte). */
+int gb_gen_path(uint32_t n, gb_csr* out);
+int gb_gen_star(uint32_t leaves, gb_csr* out);
+int gb_gen_complete(uint32_t n, gb_csr* out);
+int gb_gen_two_components(gb_csr* out);
+int gb_gen_empty(uint32_t n, gb_csr* out);
+int gb_gen_grid2d(uint32_t rows, uint32_t cols, gb_csr* out);
+int gb_gen_rmat(uint32_t scale, uint64_t edges, int directed, uint64_t seed, gb_csr* out);
+/* Benchmark-shaped graphs without a reference counterpart (new generators):
+ * road: rows x cols grid, drop_frac of edges removed, diag_frac * n random
+ *       (+-1, +-1) links, max degree <= 8;
+ * web:  directed, geometric out-degree (mean out_mean), targets by Zipf rank
+ *       popularity (in-degree exponent s), ids permuted;
+ * chung_lu: undirected, weights ~ (i + i0)^(-1/(gamma-1)), mean degree mean_deg,
+ *       w_max capped at sqrt(sum w), ids permuted. */
+int gb_gen_road(uint32_t rows, uint32_t cols, double drop_frac, double diag_frac, uint64_t seed,
+                gb_csr* out);
+int gb_gen_web(uint32_t n, double out_mean, double zipf_s, uint64_t seed, gb_csr* out);
+int gb_gen_chung_lu(uint32_t n, double gamma, double mean_deg, uint64_t seed, gb_csr* out);
+/* gbench's pickSources (src/bench/main.cpp:130-169); returns count via *k. */
+int gb_pick_sources(const gb_csr* g, int count, uint64_t seed, int any_component, uint32_t* out,
+                    int* k);
+
+/* -------------------------------------------------------------------- BFS */
+
+/* Variants: the gbench names of src/bench/main.cpp:79-81 plus new ones. */
+typedef enum {
+    GB_BFS_VERTEX = 0,     /* gpu_vertex: GpuBfs::runVertex, src/metal/bfs_gpu.mm:115 */
+    GB_BFS_NAIVE = 1,      /* gpu_naive:  runNaive,  bfs_gpu.mm:141 */
+    GB_BFS_BINNED = 2,     /* gpu_binned: runBinned, bfs_gpu.mm:177-236 */
+    GB_BFS_EDGE = 3,       /* gpu_edge:   runEdge,   bfs_gpu.mm:277-305 */
+    GB_BFS_DO = 4,         /* gpu_do:     runDO (host loop, one sync per level), bfs_gpu.mm:326-429 */
+    GB_BFS_PERSISTENT = 5  /* gpu_do_persistent: every level in one cooperative launch;
+                              also what `hybrid` (bfs_gpu.mm:307-325) maps to */
+} gb_bfs_variant;
+
+typedef enum { GB_SELECT_RULE = 0, GB_SELECT_LEARNED = 1 } gb_selector;
+
+/* Strategies a persistent-kernel level can run (the learned selector's classes). */
+typedef enum {
+    GB_STRAT_TD_EPT1 = 0, /* top-down, CTA-tiled edge-balanced expansion, 1 edge/thread/round */
+    GB_STRAT_TD_EPT2 = 1,
+    GB_STRAT_TD_EPT4 = 2,
+    GB_STRAT_TD_WARP = 3, /* top-down, warp per frontier vertex (degree-binned form) */
+    GB_STRAT_BU = 4,      /* bottom-up over the frontier bitmap */
+    GB_NUM_STRATS = 5
+} gb_strategy;
+
+/* GpuBfsOptions (src/metal/bfs_gpu.hpp:23-33) plus the new fields. */
+typedef struct {
+    uint32_t tg;         /* threads per block of the level kernels (multiple of 32, 32..1024) */
+    uint32_t small_max;  /* gpu_binned: degree <  small_max -> thread-cooperative */
+    uint32_t large_min;  /* gpu_binned: degree >= large_min -> block per vertex */
+    uint32_t ept;        /* gpu_edge / gpu_do top-down: edges per thread */
+    double alpha, beta;  /* direction rule (cpu::bfsDO, src/cpu/bfs_cpu.cpp:227-283) */
+    uint32_t selector;   /* gb_selector, persistent variant only */
+    int32_t force_strategy; /* >= 0: persistent kernel runs every level with it (profiling) */
+    uint32_t hub_min;    /* persistent: degree at which a vertex is split across blocks */
+    uint32_t block;      /* persistent / batched: threads per block (256 or 512) */
+    uint64_t spin_limit; /* grid-barrier wait bound in polls (0 = default, ~ seconds) */
+} gb_bfs_options;
+
+void gb_bfs_default_options(gb_bfs_options* o);
+
+/* util::BfsLevel (src/util/trace.hpp:7-14) plus the strategy that ran. */
+typedef struct {
+    uint32_t level;
+    char direction; /* 'T' or 'B' */
+    char device;    /* always 'G' */
+    uint8_t strategy;
+    uint8_t pad;
+    uint64_t frontier;
+    uint64_t edges;
+    double time_ms;
+} gb_level;
+
+typedef struct gb_bfs gb_bfs;
+
+/* GpuBfs(ctx, g) (src/metal/bfs_gpu.hpp:37): one upload of a symmetric CSR. */
+int gb_bfs_create(const uint32_t* row_ptr, const uint32_t* col_idx, uint64_t n, uint64_t m,
+                  gb_bfs** out);
+int gb_bfs_destroy(gb_bfs* h);
+/* GpuBfs::run* (src/metal/bfs_gpu.hpp:43-66).  out_host: n entries written on
+ * return, or NULL to leave the result in device memory (gb_bfs_device_dist).
+ * trace: optional per-level records (cap entries, *nlev = levels run). */
+int gb_bfs_run(gb_bfs* h, int variant, uint32_t source, uint32_t* out_host,
+               const gb_bfs_options* opt, gb_level* trace, size_t cap, size_t* nlev);
+/* 64-source batched BFS in one persistent launch (replaces the per-source loop
+ * of src/bench/main.cpp:324-364).  k <= 64 sources; out_host: k * n entries,
+ * source-major (out_host[i * n + v] = depth of v from sources[i]), or NULL. */
+int gb_bfs_run_batch(gb_bfs* h, const uint32_t* sources, int k, uint32_t* out_host,
+                     const gb_bfs_options* opt, gb_level* trace, size_t cap, size_t* nlev);
+/* lastGpuMs / lastLevels (src/metal/bfs_gpu.hpp:70-72): device time of the
+ * last run (CUDA events on the handle's stream) and its level count. */
+double gb_bfs_last_gpu_ms(const gb_bfs* h);
+uint32_t gb_bfs_last_levels(const gb_bfs* h);
+/* Device pointer of the last single-source result (n uint32), for callers that
+ * keep results on the GPU (GpuBfs::dist(), src/metal/bfs_gpu.hpp:40). */
+const uint32_t* gb_bfs_device_dist(const gb_bfs* h);
+/* The CUDA stream the handle launches on (cudaStream_t as void*). */
+void* gb_bfs_stream(const gb_bfs* h);
+
+/* Learned selector: load MLP parameters (layout of gb_selector_param_count) for
+ * single-source (which = 0) or batched (which = 1) persistent runs. */
+int gb_selector_shape(int* n_features, int* n_hidden, int* n_outputs);
+size_t gb_selector_param_count(void);
+int gb_bfs_set_selector(gb_bfs* h, int which, const float* params, size_t count);
+/* Selector training kernels (GPU): loss + gradient of the masked MSE over a
+ * batch (checked against the CPU oracle), and a full Adam training loop. */
+int gb_mlp_loss_grad(const float* params, int batch, const float* x, const float* y,
+                     const float* mask, float* grads_out, double* loss_out);
+int gb_mlp_forward(const float* params, int batch, const float* x, float* out);
+int gb_mlp_train(float* params_inout, int rows, const float* x, const float* y, const float* mask,
+                 int epochs, int batch, float lr, uint64_t seed, float* final_loss);
+/* Training data: run a single-source BFS level by level; at every level run
+ * each strategy from the same state, time it on the device, and record the
+ * level's features (gb_selector_shape) and the per-strategy times (us).
+ * rows_out: [cap][n_features] features, times_out: [cap][GB_NUM_STRATS].
+ * Returns the number of rows via *rows. */
+int gb_bfs_profile_levels(gb_bfs* h, uint32_t source, const gb_bfs_options* opt, int repeats,
+                          float* feats_out, float* times_out, size_t cap, size_t* rows);
+int gb_bfs_profile_batch_levels(gb_bfs* h, const uint32_t* sources, int k, const gb_bfs_options* opt,
+                                int repeats, float* feats_out, float* times_out, size_t cap,
+                                size_t* rows);
+
+/* Autotuner: pick small_max/large_min, ept, tg (and the persistent block size)
+ * per graph by timing candidates on the given sources; writes the best into *o. */
+int gb_bfs_autotune(gb_bfs* h, int variant, const uint32_t* sources, int k, gb_bfs_options* o);
+
+/* --------------------------------------------------------------- PageRank */
+
+typedef enum {
+    GB_PR_PUSH = 0,          /* gpu_push          (src/shaders/pagerank.metal:228-267) */
+    GB_PR_PULL_SCALAR = 1,   /* gpu_pull_scalar   (:306-312) */
+    GB_PR_PULL_VECTOR = 2,   /* gpu_pull_vector   (:317-327) */
+    GB_PR_PULL_ADAPTIVE = 3, /* gpu_pull_adaptive (:338-381) */
+    GB_PR_PULL_GS = 4,       /* gpu_pull_gs       (src/metal/pagerank_gpu.mm:88-192) */
+    GB_PR_PULL_F64 = 5       /* double-precision Jacobi pull: the GPU oracle for FP32 runs */
+} gb_pr_variant;
+
+/* GpuPrOptions (src/metal/pagerank_gpu.hpp:27-36). */
+typedef struct {
+    float damping;
+    int32_t iters;     /* fixed mode: iterations; tol mode: cap */
+    double tol;        /* > 0: stop when the L1 change < tol */
+    double tol_rel;    /* > 0 (tol mode): also require max relative change < tol_rel */
+    uint32_t tg;       /* threads per block of the main kernels */
+    uint32_t small_max, large_min; /* adaptive bins (in-degree) */
+    uint32_t inplace;  /* any pull variant: update contrib in place (GS-style) */
+} gb_pr_options;
+
+void gb_pr_default_options(gb_pr_options* o);
+
+/* GpuPrResult (src/metal/pagerank_gpu.hpp:38-44). */
+typedef struct {
+    int32_t iters;
+    int32_t floor_stop; /* tol mode: stopped because the L1 change stagnated */
+    double last_delta;  /* tol mode: L1 change of the last iteration (FP64 on the GPU) */
+    double last_max_rel;
+    double gpu_ms;
+} gb_pr_result;
+
+typedef struct gb_pr gb_pr;
+
+/* GpuPageRank(ctx, out, in, outdeg, needOut, needIn) (src/metal/pagerank_gpu.hpp:49-50).
+ * out_* may be NULL when the push variant is not needed, in_* when no pull is. */
+int gb_pr_create(uint64_t n, const uint32_t* out_row_ptr, const uint32_t* out_col_idx,
+                 uint64_t out_m, const uint32_t* in_row_ptr, const uint32_t* in_col_idx,
+                 uint64_t in_m, const uint32_t* outdeg, gb_pr** out);
+int gb_pr_destroy(gb_pr* h);
+/* prepareAdaptive / prepareGS (src/metal/pagerank_gpu.mm:70-192). */
+int gb_pr_prepare_adaptive(gb_pr* h, uint32_t small_max, uint32_t large_min);
+int gb_pr_prepare_gs(gb_pr* h, uint32_t pair_max_outdeg);
+/* gsColored / gsSets / gsDeferred (src/metal/pagerank_gpu.hpp:82-84). */
+int gb_pr_gs_info(const gb_pr* h, int* colored, uint64_t* sets, uint64_t* deferred);
+/* GpuPageRank::run (src/metal/pagerank_gpu.mm:336-407). */
+int gb_pr_run(gb_pr* h, int variant, const gb_pr_options* opt, gb_pr_result* res);
+/* ranks() in the caller's ids (src/metal/pagerank_gpu.mm:194-203). */
+int gb_pr_ranks(gb_pr* h, float* out_host);
+/* FP64 ranks of the last GB_PR_PULL_F64 run. */
+int gb_pr_ranks_f64(gb_pr* h, double* out_host);
+int gb_pr_autotune(gb_pr* h, gb_pr_options* o);
+void* gb_pr_stream(const gb_pr* h);
+
+/* --------------------------------------------------- primitives (tests) */
+
+/* Exclusive scan / sum / max of uint32 (src/metal/primitives.hpp:18-65),
+ * host arrays in and out; total may be NULL. */
+int gb_prim_scan(const uint32_t* in, uint64_t n, uint32_t* out, uint32_t* total);
+int gb_prim_reduce(const uint32_t* in, uint64_t n, uint32_t* sum, uint32_t* max);
+/* queueToBitmap then bitmapToQueue (src/metal/primitives.mm:103-123). */
+int gb_prim_queue_bitmap(const uint32_t* queue, uint64_t size, uint64_t n, uint32_t* bitmap_out,
+                         uint32_t* queue_out, uint64_t* count_out);
+/* Grid barrier with a wait that cannot complete (expects one more block than
+ * runs); must return GB_ERR_TIMEOUT after spin_limit polls, context intact. */
+int gb_debug_barrier_timeout(uint64_t spin_limit);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
