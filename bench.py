@@ -1,0 +1,605 @@
+"""Benchmark: exact-depth BFS on the R-MAT scale-22 power-law graph, 1 B200.
+
+Workload (one step): BFS from 64 sources picked as gbench does (largest
+component, degree > 0, seed 1; src/bench/main.cpp:155-169) on the R-MAT graph
+of 2^22 vertices and 8.5 * 2^22 drawn edges (seed 22; a=.57 b=.19 c=.19),
+symmetrised, duplicates and self-loops removed, ids permuted by reorder
+"random" seed 1: 4,194,304 vertices, 69,238,210 directed int32 edges
+(synthetic stand-in for soc-LiveJournal1).  Each BFS runs as one persistent
+cooperative launch with the learned per-level selector (alpha/beta rule when
+no trained weights ship).  GTEPS = sum over sources of the edges of the
+source's component / time (src/bench/main.cpp:329-370).
+
+  value       device-resident: graph in HBM, dist kept on the device, CUDA
+              events on the library's stream around the 64 launches.
+  e2e         the same call with a pinned host output buffer per source: the
+              16.8 MB depth array comes back to the host inside the timed region.
+  roofline    persistent kernel, HBM bound: graph-pass bytes 4(n+1)+4m+4n per
+              traversal / mean launch time, against the measured copy peak.
+  cpu_baseline the reference's own cpu_do (oracle/_ref, all host cores) on a
+              bounded sample of the same sources.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU (torchrun): replicas -- every rank runs the full 64-source step on
+its own GPU; value = all ranks' edges / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BFS GTEPS (exact); PR ms/iter & ms-to-tol 1e-6; learned vs rule-based, 1 B200"
+WORKLOAD = "rmat22_bfs64"
+SCALE, EDGES_DRAWN, GEN_SEED, PERM_SEED, NSRC = 22, 35651584, 22, 1, 64
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_graph(G, scale=SCALE, nsrc=NSRC):
+    t = time.time()
+    edges = EDGES_DRAWN if scale == SCALE else int(8.5 * (1 << scale))
+    g = G.gen.rmat(scale, edges=edges, directed=False, seed=GEN_SEED)
+    g = G.permute(g, G.random_perm(g.n, PERM_SEED))
+    srcs = G.pick_sources(g, nsrc, 1)
+    log(f"graph n={g.n} m={g.m} built in {time.time() - t:.1f}s")
+    return g, srcs
+
+
+def component_edges(g, dist):
+    deg = np.diff(g.row_ptr.astype(np.int64))
+    return int(deg[dist != 0xFFFFFFFF].sum()) // 2
+
+
+def check_depths(g, dist, src):
+    """Size-independent validity of a BFS depth array (Graph500 rules)."""
+    if dist[src] != 0:
+        return False
+    u = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(g.row_ptr.astype(np.int64)))
+    v = g.col_idx.astype(np.int64)
+    du, dv = dist[u].astype(np.int64), dist[v].astype(np.int64)
+    unr = 0xFFFFFFFF
+    if np.any((du == unr) != (dv == unr)):
+        return False
+    both = du != unr
+    if np.any(np.abs(du[both] - dv[both]) > 1):
+        return False
+    reached = np.flatnonzero(dist != unr)
+    has_parent = np.zeros(g.n, bool)
+    m = both & (dv == du - 1)
+    has_parent[u[m]] = True
+    has_parent[src] = True
+    return bool(has_parent[reached].all())
+
+
+def cpu_baseline(g, srcs, budget_s=15.0):
+    """The reference's cpu_do on all host threads (oracle/_ref), bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as O
+    if O.ref() is not None:
+        rg = O.RefGraph.of(O.HostGraph(g.n, g.m, g.flags, g.row_ptr, g.col_idx))
+        cores = int(O.ref().gref_max_threads())
+        run = lambda s: rg.bfs_do(int(s), 15.0, 18.0, threads=0, trace=False)[0]
+        kind = "reference"
+    else:
+        hg = O.HostGraph(g.n, g.m, g.flags, g.row_ptr, g.col_idx)
+        cores = 1
+        run = lambda s: O.bfs_do(hg, int(s))[0]
+        kind = "port"
+    edges, secs, used = 0, 0.0, 0
+    run(srcs[0])  # warm-up
+    t_start = time.time()
+    for s in srcs:
+        t0 = time.perf_counter()
+        d = run(s)
+        secs += time.perf_counter() - t0
+        edges += component_edges(g, d)
+        used += 1
+        if time.time() - t_start > budget_s:
+            break
+    return {"value": edges / secs / 1e9, "unit": "GTEPS", "cores": cores, "kind": kind,
+            "sample": f"cpu_do alpha=15 beta=18 from {used} of the {len(srcs)} sources, {secs:.1f}s"}
+
+
+def init_dist(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    import graph_analytics_applesilicon_b200 as G
+    g, srcs = build_graph(G)
+    per_step = 20.0 / max(1, args.steps + args.warmup)
+    for _ in range(args.warmup):
+        cpu_baseline(g, srcs, per_step)
+    vals = []
+    t0 = time.time()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(g, srcs, per_step))
+    wall = time.time() - t0
+    v = statistics.median([x["value"] for x in vals])
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GTEPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / max(1, args.steps) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "n": g.n, "m": g.m, "sources": len(srcs)},
+            "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": vals[0]["cores"], "kind": vals[0]["kind"],
+                             "sample": vals[0]["sample"]},
+            "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _timed(fn, reps=1):
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        best = min(best, time.perf_counter() - t0)
+    return best * 1e3
+
+
+def bfs_config_workload(args, world, rank, local):
+    """road_bfs: 1400 x 1400 road-shaped grid (4% of edges dropped, 0.5% diagonal
+    links, seed 1400; ~1.96M vertices, diameter > 1400 levels); 8 sources,
+    single-source persistent BFS vs the per-level plain gpu_do, plus the
+    64-source batch in one launch vs 64 plain runs.
+    chunglu_bfs64: Chung-Lu graph (3.07M vertices, gamma 2.2, mean degree 76,
+    seed 307); one 64-source batch in one launch with the learned batched
+    selector and autotuned hub cut / block size, vs 64 plain gpu_do runs."""
+    import torch
+    import graph_analytics_applesilicon_b200 as G
+    torch.cuda.set_device(local)
+    t = time.time()
+    road = args.workload == "road_bfs"
+    g = G.gen.road(1400, 1400, 0.04, 0.005, 1400) if road else G.gen.chung_lu(3070000, 2.2, 76.0, 307)
+    log(f"{args.workload}: n={g.n} m={g.m} built in {time.time() - t:.1f}s")
+    srcs64 = G.pick_sources(g, 64, 1)
+    bfs = G.GpuBfs(g)
+    comp = {int(s): component_edges(g, bfs.run("gpu_do_persistent", int(s))) for s in srcs64}
+    sel1, sel2 = G.default_selector_params("single"), G.default_selector_params("batch")
+    if sel1 is not None:
+        bfs.set_selector(sel1, 0)
+    if sel2 is not None:
+        bfs.set_selector(sel2, 1)
+    o1 = G.BfsOptions(selector="learned" if sel1 is not None else "rule")
+    ob = G.BfsOptions(selector="learned" if sel2 is not None else "rule")
+    tuned = bfs.autotune("batch", srcs64, G.BfsOptions(selector=ob.selector))
+    ob.block, ob.hub_min = tuned.block, tuned.hub_min
+    # exactness of the batch against single-source runs (size-independent)
+    d64 = bfs.run_batch(srcs64, opts=ob)
+    for i in (0, 17, 63):
+        assert np.array_equal(d64[i], bfs.run("gpu_do_persistent", int(srcs64[i]))), "batch != single"
+    valid = check_depths(g, d64[0], int(srcs64[0]))
+    for _ in range(args.warmup):
+        bfs.run_batch(srcs64, opts=ob)
+    with ClockSampler(local) as clocks:
+        batch_ms = []
+        for _ in range(args.steps):
+            bfs.run_batch(srcs64, opts=ob)
+            batch_ms.append(bfs.lastGpuMs())
+        single = srcs64[:8] if road else srcs64
+        single_ms = []
+        for s in single:
+            bfs.run("gpu_do_persistent", int(s), opts=o1)
+            single_ms.append(bfs.lastGpuMs())
+        pinned = torch.empty((64, g.n), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        e2e = _timed(lambda: bfs.run_batch(srcs64, out=pinned, opts=ob), args.steps)
+    plain = srcs64[:4] if road else srcs64[:16]
+    plain_ms = []
+    for s in plain:
+        bfs.run("gpu_do", int(s))
+        plain_ms.append(bfs.lastGpuMs())
+    plain_e2e = [_timed(lambda: bfs.run("gpu_do", int(s))) for s in plain[:2]]
+    if rank != 0:
+        return
+    e64 = sum(comp.values())
+    batch_t = statistics.median(batch_ms)
+    single_gteps = sum(comp[int(s)] for s in single) / (sum(single_ms) * 1e-3) / 1e9
+    plain_gteps = sum(comp[int(s)] for s in plain) / (sum(plain_ms) * 1e-3) / 1e9
+    value = e64 / (batch_t * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    bytes_per_trav = 4 * (g.n + 1) + 4 * g.m + 4 * g.n
+    achieved = 64 * bytes_per_trav / (batch_t * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": batch_t, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64 masks / u32 depths", "data": "synthetic",
+            "config": {"workload": args.workload, "n": g.n, "m": g.m, "sources": 64, "batch_selector": ob.selector,
+                       "tuned_block": ob.block, "tuned_hub_min": ob.hub_min, "parallelism": f"replicas{world}"},
+            "e2e": {"value": e64 / (e2e * 1e-3) / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 256,
+                    "d2h_bytes_per_step": 4 * 64 * g.n},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_kind, "kernel": "batchBfsKernel",
+                         "bytes_per_launch": 64 * bytes_per_trav, "mean_launch_ms": batch_t,
+                         "note": "graph-pass equivalents: 64 traversals per launch"},
+            "clocks": clocks.summary(), "validated": bool(valid),
+            "compare": {"batch64_one_launch_gteps": value,
+                        "single_source_persistent_gteps": single_gteps,
+                        "single_selector": o1.selector,
+                        "plain_gpu_do_gteps": plain_gteps,
+                        "plain_gpu_do_ms_per_source": statistics.mean(plain_ms),
+                        "plain_gpu_do_e2e_ms_per_source": statistics.mean(plain_e2e),
+                        "persistent_ms_per_source": statistics.mean(single_ms),
+                        "speedup_persistent_vs_plain": statistics.mean(plain_ms) / statistics.mean(single_ms),
+                        "speedup_batch_vs_64_plain": 64 * statistics.mean(plain_ms) / batch_t}}
+    print(json.dumps(line), flush=True)
+
+
+def pagerank_tol_workload(args, world, rank, local):
+    """Web-shaped directed graph (875,000 vertices, geometric out-degree mean
+    5.8 -> ~15% dangling, Zipf s=2.1 in-degree, seed 875): PageRank to tol 1e-6,
+    Jacobi (degree-adaptive pull) vs in-place Gauss-Seidel (pair deferral K=2),
+    FP32 against the FP64 GPU oracle.  value: ms to tol of the faster method
+    that meets its accuracy rule."""
+    import torch
+    import graph_analytics_applesilicon_b200 as G
+    torch.cuda.set_device(local)
+    g = G.gen.web(875000, 5.8, 2.1, 875)
+    gin = G.transpose(g)
+    pr = G.GpuPageRank(g.n, g, gin, g.degrees())
+    pr.prepareGS(2)
+    o = G.PrOptions(tol=1e-6, iters=1000)
+    pr.run("gpu_pull_f64", o)
+    ref_jac = pr.ranks_f64()
+    pr.run("gpu_pull_f64", G.PrOptions(tol=1e-12, iters=2000))
+    conv = pr.ranks_f64()
+    res = {}
+    for v in ("gpu_pull_adaptive", "gpu_pull_vector", "gpu_pull_gs"):
+        for _ in range(args.warmup):
+            pr.run(v, o)
+        ts = []
+        for _ in range(args.steps):
+            r = pr.run(v, o)
+            ts.append(r.gpu_ms)
+        got = pr.ranks().astype(np.float64)
+        res[v] = {"ms_to_tol": statistics.median(ts), "iters": r.iters, "last_delta": r.last_delta,
+                  "l1_vs_fp64_same_method": float(np.abs(got - ref_jac).sum()),
+                  "l1_vs_converged": float(np.abs(got - conv).sum()), "sum": float(got.sum())}
+    jac_l1 = float(np.abs(ref_jac - conv).sum())
+    gs_ok = res["gpu_pull_gs"]["l1_vs_converged"] <= max(1e-4, jac_l1)
+    best = "gpu_pull_gs" if gs_ok and res["gpu_pull_gs"]["ms_to_tol"] < res["gpu_pull_adaptive"]["ms_to_tol"] \
+        else "gpu_pull_adaptive"
+    if rank != 0:
+        return
+    out = torch.empty(g.n, dtype=torch.float32, pin_memory=True).numpy()
+    e2e = _timed(lambda: (pr.run(best, o), G.check(G.lib().gb_pr_ranks(pr._h, out))), 3)
+    line = {"metric": METRIC, "value": res[best]["ms_to_tol"], "unit": "ms to tol 1e-6", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[best]["ms_to_tol"],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 residual)",
+            "data": "synthetic", "config": {"workload": "web_pr_tol", "n": g.n, "m": g.m, "method": best},
+            "e2e": {"value": e2e, "unit": "ms to tol 1e-6", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4 * g.n},
+            "gpu_launches": None, "results": res, "fp64_jacobi_vs_converged_l1": jac_l1, "gs_accuracy_ok": gs_ok}
+    print(json.dumps(line), flush=True)
+
+
+def pagerank_workload(args, world, rank, local):
+    """Chung-Lu graph (3.07M vertices, gamma 2.2, mean degree 76, seed 307, ids
+    permuted): 20 fixed Jacobi iterations of the degree-adaptive pull in FP32,
+    one step = one 20-iteration run (a CUDA-graph replay), ms per iteration.
+    Checked against the double-precision GPU pull at L1 < 1e-4."""
+    import torch
+    import graph_analytics_applesilicon_b200 as G
+    torch.cuda.set_device(local)
+    t = time.time()
+    g = G.gen.chung_lu(args.n, 2.2, 76.0, 307)
+    log(f"chung-lu n={g.n} m={g.m} built in {time.time() - t:.1f}s")
+    pr = G.GpuPageRank(g.n, g, g, g.degrees())  # undirected: out-CSR = in-CSR
+    o = G.PrOptions(iters=20)
+    pr.run("gpu_pull_f64", o)
+    ref = pr.ranks_f64()
+    pr.run("gpu_pull_adaptive", o)
+    got = pr.ranks().astype(np.float64)
+    l1 = float(np.abs(got - ref).sum())
+    stream = torch.cuda.ExternalStream(G.lib().gb_pr_stream(pr._h))
+    for _ in range(args.warmup):
+        pr.run("gpu_pull_adaptive", o)
+    barrier = (lambda: (__import__("torch.distributed").distributed.barrier(), torch.cuda.synchronize())) \
+        if world > 1 else torch.cuda.synchronize
+    barrier()
+    with ClockSampler(local) as clocks:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        gpu = []
+        ev0.record(stream)
+        for _ in range(args.steps):
+            r = pr.run("gpu_pull_adaptive", o)
+            gpu.append(r.gpu_ms)
+        ev1.record(stream)
+        ev1.synchronize()
+        total = ev0.elapsed_time(ev1)
+        e2e = []
+        out = torch.empty(g.n, dtype=torch.float32, pin_memory=True).numpy()
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            pr.run("gpu_pull_adaptive", o)
+            G.check(G.lib().gb_pr_ranks(pr._h, out))
+            e2e.append((time.perf_counter() - t0) * 1e3)
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([total, sum(e2e)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total, e2e_sum = tt.tolist()
+    else:
+        e2e_sum = sum(e2e)
+    compare = {}
+    for v in ("gpu_pull_vector", "gpu_pull_scalar", "gpu_push"):
+        rr = [pr.run(v, o).gpu_ms for _ in range(2)]
+        compare[v + "_ms_per_iter"] = min(rr) / 20
+    if rank != 0:
+        return
+    ms_iter = total / args.steps / 20
+    peak, peak_kind = peaks()
+    bytes_sweep = 4 * (g.n + 1) + 8 * g.m + 4 * g.n
+    kernel_ms = statistics.mean(gpu) / 20
+    achieved = bytes_sweep / (kernel_ms * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle_py as O
+            if O.ref() is not None:
+                rg = O.RefGraph.of(O.HostGraph(g.n, g.m, g.flags, g.row_ptr, g.col_idx))
+                t0 = time.perf_counter()
+                rg.pagerank(g.degrees(), 2, 0.0, threads=0)
+                sec = time.perf_counter() - t0
+                cpu = {"value": sec * 1e3 / 2, "unit": "ms/iter", "cores": int(O.ref().gref_max_threads()),
+                       "kind": "reference", "sample": "cpu_omp (dynamic,256), 2 iterations on the full graph"}
+        except Exception as e:
+            cpu = {"value": None, "error": str(e)[:200]}
+    line = {"metric": METRIC, "value": ms_iter, "unit": "ms/iter", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total / args.steps, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "chunglu_pr20", "n": g.n, "m": g.m, "variant": "gpu_pull_adaptive",
+                       "iters": 20, "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (in-CSR 947 MB)"},
+            "e2e": {"value": e2e_sum / args.steps / 20, "unit": "ms/iter", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 4 * g.n},
+            "gpu_launches": 21 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_kind, "kernel": "prPullKernel<2,false>",
+                         "bytes_per_launch": bytes_sweep, "mean_launch_ms": kernel_ms},
+            "cpu_baseline": cpu, "clocks": clocks.summary(),
+            "accuracy": {"l1_vs_fp64_gpu": l1, "ok": l1 < 1e-4}, "compare": compare}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain/rule comparison runs")
+    ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (smaller: profiling cases)")
+    ap.add_argument("--sources", type=int, default=NSRC)
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=[WORKLOAD, "chunglu_pr20", "road_bfs", "chunglu_bfs64", "web_pr_tol"],
+                    help="rmat22_bfs64 (default, the headline); chunglu_pr20, road_bfs, chunglu_bfs64, web_pr_tol")
+    ap.add_argument("--n", type=int, default=3070000, help="chunglu_pr20: vertices")
+    args = ap.parse_args()
+    world, rank, local = init_dist(args)
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+        return
+    args.warmup = max(3, args.warmup)
+    if args.workload == "chunglu_pr20":
+        pagerank_workload(args, world, rank, local)
+        return
+    if args.workload in ("road_bfs", "chunglu_bfs64"):
+        bfs_config_workload(args, world, rank, local)
+        return
+    if args.workload == "web_pr_tol":
+        pagerank_tol_workload(args, world, rank, local)
+        return
+
+    import torch
+    import graph_analytics_applesilicon_b200 as G
+    torch.cuda.set_device(local)
+    g, srcs = build_graph(G, args.scale, args.sources)
+    bfs = G.GpuBfs(g)
+    sel = G.default_selector_params("single")
+    selector = "rule"
+    if sel is not None:
+        bfs.set_selector(sel, 0)
+        selector = "learned"
+    opts = G.BfsOptions(selector=selector)
+    stream = torch.cuda.ExternalStream(G.lib().gb_bfs_stream(bfs._h))
+
+    # exactness of one result (size-independent check) and TEPS denominators
+    comp = []
+    d0 = None
+    for i, s in enumerate(srcs):
+        d = bfs.run("gpu_do_persistent", int(s), opts=opts)
+        comp.append(component_edges(g, d))
+        if i == 0:
+            d0 = d.copy()
+    valid = check_depths(g, d0, int(srcs[0]))
+    edges_per_step = sum(comp)
+
+    def device_step(variant="gpu_do_persistent", o=opts):
+        ms = []
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for s in srcs:
+            G.check(G.lib().gb_bfs_run(bfs._h, G.BFS_VARIANTS[variant], int(s), None, G.C.byref(o), None, 0, None))
+            ms.append(G.lib().gb_bfs_last_gpu_ms(bfs._h))
+        ev1.record(stream)
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1), ms
+
+    pinned = torch.empty(g.n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+
+    def e2e_step():
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s in srcs:
+            G.check(G.lib().gb_bfs_run(bfs._h, 5, int(s), pinned.ctypes.data, G.C.byref(opts), None, 0, None))
+        return (time.perf_counter() - t0) * 1e3
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        device_step()
+        e2e_step()
+    barrier()
+    with ClockSampler(local) as clocks:
+        step_ms, launch_ms = [], []
+        for _ in range(args.steps):
+            t, ms = device_step()
+            step_ms.append(t)
+            launch_ms += ms
+        barrier()
+        e2e_ms = [e2e_step() for _ in range(args.steps)]
+        barrier()
+    total_ms = sum(step_ms)
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([total_ms, e2e_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms, e2e_total = tt.tolist()
+
+    # comparison forms on the same sources (not part of the timed region)
+    plain_ms = rule_ms = float("nan")
+    if not args.no_compare:
+        plain_ms = device_step("gpu_do", G.BfsOptions())[0]
+        rule_ms = device_step("gpu_do_persistent", G.BfsOptions(selector="rule"))[0]
+    # reference summary: harmonic mean over sources of per-source GTEPS (src/bench/main.cpp:366-370)
+    hmean = len(srcs) / sum((lm * 1e-3) / (c / 1e9) for lm, c in zip(launch_ms[: len(srcs)], comp) if c)
+
+    peak, peak_kind = peaks()
+    bytes_per_trav = 4 * (g.n + 1) + 4 * g.m + 4 * g.n
+    mean_launch = statistics.mean(launch_ms)
+    achieved = bytes_per_trav / (mean_launch * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "persistent_bfs_rmat22_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    value = world * edges_per_step * args.steps / (total_ms * 1e-3) / 1e9
+    e2e_value = world * edges_per_step * args.steps / (e2e_total * 1e-3) / 1e9
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            cpu = cpu_baseline(g, srcs)
+        except Exception as e:  # reported, never fatal
+            cpu = {"value": None, "error": str(e)[:200]}
+    line = {
+        "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": WORKLOAD if args.scale == SCALE else f"rmat{args.scale}_bfs{len(srcs)}", "n": g.n, "m": g.m, "sources": len(srcs), "selector": selector,
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (CSR 293 MB)",
+                   "edges_per_step": edges_per_step},
+        "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),
+                "d2h_bytes_per_step": 4 * g.n * len(srcs)},
+        "gpu_launches": len(srcs) * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "kernel": "persistentBfsKernel<512>", "bytes_per_launch": bytes_per_trav,
+                     "mean_launch_ms": mean_launch},
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+        "validated": bool(valid),
+        "compare": {"plain_gpu_do_gteps": edges_per_step / (plain_ms * 1e-3) / 1e9,
+                    "persistent_rule_gteps": edges_per_step / (rule_ms * 1e-3) / 1e9,
+                    "speedup_vs_plain_gpu_do": plain_ms / (total_ms / args.steps),
+                    "hmean_gteps_per_source": hmean},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -25,7 +25,7 @@ FLAG_DIRECTED, FLAG_SORTED, FLAG_DEDUP = 1, 2, 4
 
 # gb_bfs_variant / gb_strategy / gb_pr_variant (include/graph_b200.h)
 BFS_VARIANTS = {"gpu_vertex": 0, "gpu_naive": 1, "gpu_binned": 2, "gpu_edge": 3, "gpu_do": 4,
-                "gpu_do_persistent": 5, "hybrid": 5}
+                "gpu_do_persistent": 5, "hybrid": 5, "batch": 6}
 STRATEGIES = ["td_ept1", "td_ept2", "td_ept4", "td_warp", "bu"]
 PR_VARIANTS = {"gpu_push": 0, "gpu_pull_scalar": 1, "gpu_pull_vector": 2, "gpu_pull_adaptive": 3,
                "gpu_pull_gs": 4, "gpu_pull_f64": 5}
@@ -409,6 +409,18 @@ class GpuBfs:
         rows = C.c_size_t(0)
         o = opts if opts is not None else BfsOptions()
         check(lib().gb_bfs_profile_levels(self._h, source, C.byref(o), repeats, feats, times, cap, C.byref(rows)))
+        return feats[: rows.value], times[: rows.value]
+
+    def profile_batch_levels(self, sources, opts: BfsOptions | None = None, repeats: int = 3):
+        nf = selector_shape()[0]
+        cap = 1 << 16
+        feats = np.zeros((cap, nf), np.float32)
+        times = np.zeros((cap, len(STRATEGIES)), np.float32)
+        rows = C.c_size_t(0)
+        src = np.ascontiguousarray(sources, np.uint32)
+        o = opts if opts is not None else BfsOptions()
+        check(lib().gb_bfs_profile_batch_levels(self._h, src, src.size, C.byref(o), repeats, feats, times, cap,
+                                                C.byref(rows)))
         return feats[: rows.value], times[: rows.value]
 
     def autotune(self, variant, sources, opts: BfsOptions | None = None) -> BfsOptions:

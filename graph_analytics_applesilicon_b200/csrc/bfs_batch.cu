@@ -1,0 +1,598 @@
+// bfs_batch.cu -- up to 64 BFS sources in one persistent cooperative launch.
+//
+// Replaces the reference's one-source-at-a-time loop (src/bench/main.cpp:324-364).
+// Bit i of a vertex's 64-bit masks stands for source i:
+//   seen[v]    sources that have reached v;
+//   fr[2][v]   sources whose frontier v is on at the current / next level;
+//   nx[v]      bits pushed to v during a top-down level (zero between levels).
+// Active vertices (fr != 0) are kept in a queue (vertex, adjacency start,
+// degree) and a hub list for degree >= hub_min, as in the single-source kernel.
+// A level runs top-down (push: bits = fr[u] & ~seen[v], atomicOr into nx[v];
+// the first pusher of v appends it to a candidate list; after a grid barrier
+// the candidates' new bits are folded into seen / fr / depths) or bottom-up
+// (pull: every vertex still missing sources ORs its neighbours' frontier masks
+// until it has them all).  The direction rule of cpu::bfsDO
+// (src/cpu/bfs_cpu.cpp:227-283) runs on the batch's counters (active vertices
+// and their edges), or the learned selector picks; depths are the same either
+// way.  Depths: dist[i*n + v]; unreached entries are written once at the end.
+#include <algorithm>
+#include <cstring>
+
+#include "bfs.hpp"
+#include "bfs_device.cuh"
+
+namespace gb {
+namespace {
+
+constexpr unsigned long long kHubShift = 40;
+constexpr unsigned long long kHubMask = (1ull << kHubShift) - 1;
+constexpr uint32_t kTraceCap = 1u << 16;
+
+struct BCounters {
+    unsigned acnt;                 // next active queue entries
+    unsigned ccnt;                 // top-down candidates
+    unsigned work[2];              // work tickets: expansion, finalisation
+    unsigned long long hubPack;    // next active hubs: (count << 40) | degree sum
+    unsigned long long aedges;     // degree sum of the next active vertices
+    unsigned long long found;      // next active vertices
+    unsigned long long bits;       // newly set (vertex, source) pairs
+    unsigned long long fullEdges;  // degree sum of vertices that became fully seen
+    unsigned long long fullCount;
+    unsigned long long examined;
+};
+
+struct BArgs {
+    const uint32_t* __restrict__ row_ptr;
+    const uint32_t* __restrict__ col_idx;
+    unsigned long long* seen;
+    unsigned long long* fr[2];
+    unsigned long long* nx;
+    uint32_t* qv[2];
+    uint32_t* qs[2];
+    uint32_t* qd[2];
+    uint32_t* hv[2];
+    uint32_t* hs[2];
+    unsigned long long* ho[2];
+    uint32_t* cq;
+    uint32_t* dist;
+    const uint32_t* sources;
+    BCounters* ctr;
+    unsigned* ctl;
+    gb_level* trace;
+    const float* sel;
+    uint64_t n, m;
+    unsigned long long all;
+    int k;
+    uint32_t hubMin, traceCap;
+    double alpha, beta;
+    int selector, force;
+    unsigned long long spinLimit;
+};
+
+__device__ __forceinline__ unsigned long long ldv64(const unsigned long long* p) {
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+__device__ __forceinline__ unsigned ldv32(const unsigned* p) { return *reinterpret_cast<const volatile unsigned*>(p); }
+
+__device__ __forceinline__ unsigned long long warpOr64(unsigned long long x) {
+    unsigned lo = __reduce_or_sync(kFull, (unsigned)x), hi = __reduce_or_sync(kFull, (unsigned)(x >> 32));
+    return ((unsigned long long)hi << 32) | lo;
+}
+
+struct BAcc {
+    unsigned long long found = 0, aedges = 0, bits = 0, fullEdges = 0, fullCount = 0, exam = 0;
+};
+
+template <int NT>
+struct BSmem {
+    uint32_t scan[NT / 32 + 1];
+    uint32_t off[NT];
+    uint32_t st[NT];
+    unsigned long long f[NT];
+    float sel[kSelParams];
+    unsigned long long acc[6];
+    uint32_t range[2];
+    unsigned item;
+    int strat;
+    uint32_t base;
+};
+
+// Write depth `level` for the sources in b (lanes of a warp call together;
+// consecutive vertices give coalesced stores per source).
+__device__ __forceinline__ void writeDepths(const BArgs& a, uint64_t v, unsigned long long b, uint32_t value) {
+    unsigned long long any = warpOr64(b);
+    while (any) {
+        const int s = __ffsll((long long)any) - 1;
+        any &= any - 1;
+        if ((b >> s) & 1ull) a.dist[(uint64_t)s * a.n + v] = value;
+    }
+}
+
+// Block-aggregated append of vertex v (with its adjacency start and degree)
+// to the next active queue or hub list.  All threads of the block call it.
+template <int NT>
+__device__ __forceinline__ void appendActive(const BArgs& a, BSmem<NT>& sm, bool want, uint32_t v, uint32_t st,
+                                             uint32_t d, uint32_t nq, BCounters* cur) {
+    const bool hub = want && d >= a.hubMin;
+    const bool q = want && !hub;
+    uint32_t tot;
+    const uint32_t pos = blockScan<NT>(q ? 1u : 0u, &tot, sm.scan);
+    if (threadIdx.x == 0) sm.base = tot ? atomicAdd(&cur->acnt, tot) : 0u;
+    __syncthreads();
+    if (q) {
+        const uint32_t p = sm.base + pos;
+        a.qv[nq][p] = v;
+        a.qs[nq][p] = st;
+        a.qd[nq][p] = d;
+    }
+    if (hub) {
+        const unsigned long long old = atomicAdd(&cur->hubPack, (1ull << kHubShift) | d);
+        const uint32_t i = (uint32_t)(old >> kHubShift);
+        a.hv[nq][i] = v;
+        a.hs[nq][i] = st;
+        a.ho[nq][i] = old & kHubMask;
+    }
+    __syncthreads();
+}
+
+// Fold new bits b into v (owner thread only): seen, next frontier, depths
+// (by the caller, warp-wide), counters.
+__device__ __forceinline__ void foldBits(const BArgs& a, uint64_t v, unsigned long long old,
+                                         unsigned long long b, uint32_t d, BAcc& acc) {
+    a.seen[v] = old | b;
+    acc.found++;
+    acc.aedges += d;
+    acc.bits += __popcll(b);
+    if ((old | b) == a.all) {
+        acc.fullEdges += d;
+        acc.fullCount++;
+    }
+}
+
+// Top-down push of one tile of NT active entries (edge-balanced, as the
+// single-source kernel): the entry's frontier mask minus the target's seen
+// mask is ORed into nx[target]; the first pusher records a candidate.
+template <int NT, int EPT>
+__device__ void pushTile(const BArgs& a, BSmem<NT>& sm, uint32_t item, uint32_t S, uint32_t qc, BCounters* cur) {
+    const uint32_t idx = item * NT + threadIdx.x;
+    uint32_t st = 0, d = 0;
+    unsigned long long f = 0;
+    if (idx < S) {
+        st = a.qs[qc][idx];
+        d = a.qd[qc][idx];
+        f = a.fr[qc][a.qv[qc][idx]];
+    }
+    uint32_t tot;
+    const uint32_t off = blockScan<NT>(d, &tot, sm.scan);
+    sm.off[threadIdx.x] = off;
+    sm.st[threadIdx.x] = st;
+    sm.f[threadIdx.x] = f;
+    __syncthreads();
+    const uint32_t cnt = min((uint32_t)NT, S - item * NT);
+    for (uint32_t base = 0; base < tot; base += NT * EPT) {
+        uint32_t u[EPT];
+        unsigned long long fu[EPT];
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const uint32_t e = base + k * NT + threadIdx.x;
+            u[k] = 0;
+            fu[k] = 0;
+            if (e < tot) {
+                const uint32_t o = ownerOf(sm.off, 0u, cnt - 1, e);
+                u[k] = a.col_idx[sm.st[o] + (e - sm.off[o])];
+                fu[k] = sm.f[o];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            bool cand = false;
+            if (fu[k]) {
+                const unsigned long long bits = fu[k] & ~a.seen[u[k]];
+                if (bits) cand = atomicOr(&a.nx[u[k]], bits) == 0ull;
+            }
+            if (__any_sync(kFull, cand)) {
+                const uint32_t pos = warpAppend(cand, &cur->ccnt);
+                if (cand) a.cq[pos] = u[k];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int NT>
+__device__ void pushWarpItem(const BArgs& a, uint32_t item, uint32_t S, uint32_t qc, BCounters* cur) {
+    const uint32_t idx = item * (NT / 32) + (threadIdx.x >> 5);
+    if (idx >= S) return;  // warp-uniform
+    const uint32_t st = a.qs[qc][idx], d = a.qd[qc][idx];
+    const unsigned long long f = a.fr[qc][a.qv[qc][idx]];
+    for (uint32_t base = 0; base < d; base += 32) {
+        const uint32_t e = base + laneId();
+        bool cand = false;
+        if (e < d) {
+            const uint32_t u = a.col_idx[st + e];
+            const unsigned long long bits = f & ~a.seen[u];
+            if (bits && atomicOr(&a.nx[u], bits) == 0ull) {
+                cand = true;
+                const uint32_t pos = atomicAdd(&cur->ccnt, 1u);
+                a.cq[pos] = u;
+            }
+        }
+        (void)cand;
+    }
+}
+
+template <int NT>
+__device__ void pushHubChunk(const BArgs& a, BSmem<NT>& sm, uint64_t e0, uint64_t e1, uint32_t H, uint32_t qc,
+                             BCounters* cur) {
+    const unsigned long long* ho = a.ho[qc];
+    if (threadIdx.x == 0) {
+        const uint32_t lo = ownerOf(ho, 0u, H - 1, (unsigned long long)e0);
+        sm.range[0] = lo;
+        sm.range[1] = ownerOf(ho, lo, H - 1, (unsigned long long)(e1 - 1));
+    }
+    __syncthreads();
+    const uint32_t lo = sm.range[0], hi = sm.range[1];
+    for (uint64_t base = e0; base < e1; base += NT) {
+        const uint64_t e = base + threadIdx.x;
+        bool cand = false;
+        uint32_t u = 0;
+        if (e < e1) {
+            const uint32_t o = ownerOf(ho, lo, hi, (unsigned long long)e);
+            u = a.col_idx[a.hs[qc][o] + (uint32_t)(e - ho[o])];
+            const unsigned long long bits = a.fr[qc][a.hv[qc][o]] & ~a.seen[u];
+            if (bits) cand = atomicOr(&a.nx[u], bits) == 0ull;
+        }
+        if (__any_sync(kFull, cand)) {
+            const uint32_t pos = warpAppend(cand, &cur->ccnt);
+            if (cand) a.cq[pos] = u;
+        }
+    }
+    __syncthreads();
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
+    __shared__ BSmem<NT> sm;
+    const unsigned tid = threadIdx.x;
+    const uint64_t gtid = (uint64_t)blockIdx.x * NT + tid, gthreads = (uint64_t)gridDim.x * NT;
+    unsigned* bar = &a.ctl[0];
+    unsigned* err = &a.ctl[1];
+    const bool learned = a.selector == GB_SELECT_LEARNED && a.sel != nullptr;
+    if (learned)
+        for (int i = tid; i < kSelParams; i += NT) sm.sel[i] = a.sel[i];
+
+    // prologue: masks zeroed, counters zeroed, then the sources
+    for (uint64_t v = gtid; v < a.n; v += gthreads) {
+        a.seen[v] = 0;
+        a.fr[0][v] = 0;
+        a.fr[1][v] = 0;
+        a.nx[v] = 0;
+    }
+    if (gtid == 0)
+        for (int s = 0; s < 4; ++s) a.ctr[s] = BCounters{};
+    if (!gridBarrier(bar, err, a.spinLimit)) return;
+    if (blockIdx.x == 0 && tid < (unsigned)a.k) {
+        const uint32_t v = a.sources[tid];
+        const unsigned long long bit = 1ull << tid;
+        const unsigned long long old = atomicOr(&a.fr[0][v], bit);
+        atomicOr(&a.seen[v], bit);
+        a.dist[(uint64_t)tid * a.n + v] = 0;
+        BCounters* c = &a.ctr[3];
+        atomicAdd(&c->bits, 1ull);
+        if (old == 0) {  // first source at v: v becomes active
+            const uint32_t st = a.row_ptr[v], d = a.row_ptr[v + 1] - st;
+            atomicAdd(&c->found, 1ull);
+            atomicAdd(&c->aedges, (unsigned long long)d);
+            if (d >= a.hubMin) {
+                const unsigned long long o = atomicAdd(&c->hubPack, (1ull << kHubShift) | d);
+                const uint32_t i = (uint32_t)(o >> kHubShift);
+                a.hv[0][i] = v;
+                a.hs[0][i] = st;
+                a.ho[0][i] = o & kHubMask;
+            } else {
+                const uint32_t p = atomicAdd(&c->acnt, 1u);
+                a.qv[0][p] = v;
+                a.qs[0][p] = st;
+                a.qd[0][p] = d;
+            }
+        }
+    }
+    if (!gridBarrier(bar, err, a.spinLimit)) return;
+
+    uint32_t level = 0;
+    bool bottomUp = false;
+    uint64_t scout = ldv64(&a.ctr[3].aedges), toCheck = a.m, fullEdges = 0, fullCount = 0;
+    int lastStrat = -1;
+    uint64_t tPrev = globaltimer();
+    for (;;) {
+        BCounters* prev = &a.ctr[(level + 3) & 3];
+        BCounters* prev2 = &a.ctr[(level + 2) & 3];
+        BCounters* cur = &a.ctr[level & 3];
+        const uint64_t size = ldv64(&prev->found), fedges = ldv64(&prev->aedges);
+        if (size == 0) break;
+        if (!bottomUp && (double)scout > (double)toCheck / a.alpha) bottomUp = true;
+        if (!bottomUp) toCheck -= min(toCheck, scout);
+        const int ruleStrat = bottomUp ? GB_STRAT_BU : GB_STRAT_TD_EPT2;
+        int strat = ruleStrat;
+        if (a.force >= 0) {
+            strat = a.force;
+        } else if (learned) {
+            if (tid < 32) {
+                float f[kSelFeatures];
+                selectorFeatures((double)size, (double)fedges, (double)(a.m > fullEdges ? a.m - fullEdges : 0),
+                                 (double)(a.n - fullCount), (double)a.n, (double)a.m, (double)level, f);
+                const int s = selectorArgmin(sm.sel, f, tid);
+                if (tid == 0) sm.strat = s;
+            }
+            __syncthreads();
+            if (sm.strat >= 0) strat = sm.strat;
+        }
+        if (gtid == 0) {
+            if (a.trace && level > 0 && level - 1 < a.traceCap && lastStrat == GB_STRAT_BU)
+                a.trace[level - 1].edges = ldv64(&prev->examined);
+            if (a.trace && level < a.traceCap) {
+                gb_level r;
+                r.level = level;
+                r.direction = strat == GB_STRAT_BU ? 'B' : 'T';
+                r.device = 'G';
+                r.strategy = (uint8_t)strat;
+                r.pad = (uint8_t)ruleStrat;
+                r.frontier = size;
+                r.edges = fedges;
+                r.time_ms = 0;
+                a.trace[level] = r;
+            }
+            a.ctr[(level + 1) & 3] = BCounters{};
+        }
+        if (tid == 0)
+            for (int i = 0; i < 6; ++i) sm.acc[i] = 0;
+        __syncthreads();
+        const uint32_t qc = level & 1u, nq = qc ^ 1u;
+        BAcc acc;
+        if (strat == GB_STRAT_BU) {
+            const unsigned long long* fc = a.fr[qc];
+            for (uint64_t base = (uint64_t)blockIdx.x * NT; base < a.n; base += gthreads) {
+                const uint64_t v = base + tid;
+                unsigned long long b = 0, old = 0;
+                uint32_t st = 0, d = 0;
+                if (v < a.n) {
+                    old = a.seen[v];
+                    const unsigned long long need = a.all & ~old;
+                    st = a.row_ptr[v];
+                    d = a.row_ptr[v + 1] - st;
+                    if (need) {
+                        // OR the neighbours' frontier masks until every missing
+                        // source is covered; aligned groups of 4 entries are
+                        // loaded at once with their 4 masks.
+                        unsigned long long got = 0;
+                        uint32_t i = st;
+                        const uint32_t e = st + d;
+                        for (; i < e && (i & 3u) && (got & need) != need; ++i) got |= fc[a.col_idx[i]];
+                        for (; i + 4 <= e && (got & need) != need; i += 4) {
+                            const uint4 q = *reinterpret_cast<const uint4*>(a.col_idx + i);
+                            got |= fc[q.x] | fc[q.y] | fc[q.z] | fc[q.w];
+                        }
+                        for (; i < e && (got & need) != need; ++i) got |= fc[a.col_idx[i]];
+                        acc.exam += i - st;
+                        b = got & need;
+                    }
+                    a.fr[nq][v] = b;  // dense: also clears the level-before-last frontier
+                    if (b) foldBits(a, v, old, b, d, acc);
+                }
+                writeDepths(a, v, b, level + 1);
+                appendActive<NT>(a, sm, b != 0, (uint32_t)v, st, d, nq, cur);
+            }
+        } else {
+            // phase A: clear the previous level's frontier entries of fr[nq]
+            // (its active list is still intact), then push.
+            {
+                const uint32_t P = ldv32(&prev2->acnt);
+                for (uint64_t i = gtid; i < P; i += gthreads) a.fr[nq][a.qv[nq][i]] = 0;
+                const uint32_t PH = (uint32_t)(ldv64(&prev2->hubPack) >> kHubShift);
+                for (uint64_t i = gtid; i < PH; i += gthreads) a.fr[nq][a.hv[nq][i]] = 0;
+            }
+            const uint32_t S = ldv32(&prev->acnt);
+            const unsigned long long hp = ldv64(&prev->hubPack);
+            const uint32_t H = (uint32_t)(hp >> kHubShift);
+            const uint64_t HE = hp & kHubMask;
+            const uint32_t per = strat == GB_STRAT_TD_WARP ? NT / 32 : NT;
+            const uint32_t nt = (S + per - 1) / per;
+            const uint64_t HC = (uint64_t)NT * 4;
+            const uint32_t nh = (uint32_t)((HE + HC - 1) / HC);
+            for (bool first = true;; first = false) {  // block b takes item b first
+                if (tid == 0) sm.item = first ? blockIdx.x : gridDim.x + atomicAdd(&cur->work[0], 1u);
+                __syncthreads();
+                const uint32_t item = sm.item;
+                __syncthreads();
+                if (item >= nt + nh) break;
+                if (item < nt) {
+                    switch (strat) {
+                        case GB_STRAT_TD_EPT1: pushTile<NT, 1>(a, sm, item, S, qc, cur); break;
+                        case GB_STRAT_TD_EPT4: pushTile<NT, 4>(a, sm, item, S, qc, cur); break;
+                        case GB_STRAT_TD_WARP: pushWarpItem<NT>(a, item, S, qc, cur); break;
+                        default: pushTile<NT, 2>(a, sm, item, S, qc, cur); break;
+                    }
+                } else {
+                    const uint64_t e0 = (uint64_t)(item - nt) * HC;
+                    pushHubChunk<NT>(a, sm, e0, min(e0 + HC, HE), H, qc, cur);
+                }
+            }
+            if (!gridBarrier(bar, err, a.spinLimit)) return;
+            // phase B: fold the candidates' pushed bits
+            const uint32_t C = ldv32(&cur->ccnt);
+            for (uint64_t base = (uint64_t)blockIdx.x * NT; base < C; base += gthreads) {
+                const uint64_t i = base + tid;
+                unsigned long long b = 0;
+                uint32_t v = 0, st = 0, d = 0;
+                if (i < C) {
+                    v = a.cq[i];
+                    const unsigned long long old = a.seen[v];
+                    b = a.nx[v] & ~old;
+                    a.nx[v] = 0;
+                    if (b) {
+                        st = a.row_ptr[v];
+                        d = a.row_ptr[v + 1] - st;
+                        a.fr[nq][v] = b;
+                        foldBits(a, v, old, b, d, acc);
+                        unsigned long long bb = b;
+                        while (bb) {
+                            const int s = __ffsll((long long)bb) - 1;
+                            bb &= bb - 1;
+                            a.dist[(uint64_t)s * a.n + v] = level + 1;
+                        }
+                    }
+                }
+                appendActive<NT>(a, sm, b != 0, v, st, d, nq, cur);
+            }
+        }
+        // counters: one atomic per block and counter
+        unsigned long long vals[6] = {acc.found, acc.aedges, acc.bits, acc.fullEdges, acc.fullCount, acc.exam};
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const unsigned long long x = warpSum(vals[i]);
+            if (laneId() == 0 && x) atomicAdd(&sm.acc[i], x);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            if (sm.acc[0]) atomicAdd(&cur->found, sm.acc[0]);
+            if (sm.acc[1]) atomicAdd(&cur->aedges, sm.acc[1]);
+            if (sm.acc[2]) atomicAdd(&cur->bits, sm.acc[2]);
+            if (sm.acc[3]) atomicAdd(&cur->fullEdges, sm.acc[3]);
+            if (sm.acc[4]) atomicAdd(&cur->fullCount, sm.acc[4]);
+            if (sm.acc[5]) atomicAdd(&cur->examined, sm.acc[5]);
+        }
+        if (!gridBarrier(bar, err, a.spinLimit)) return;
+        if (gtid == 0) {
+            const uint64_t t = globaltimer();
+            if (a.trace && level < a.traceCap) a.trace[level].time_ms = (double)(t - tPrev) * 1e-6;
+            tPrev = t;
+        }
+        const uint64_t found = ldv64(&cur->found), nextE = ldv64(&cur->aedges);
+        fullEdges += ldv64(&cur->fullEdges);
+        fullCount += ldv64(&cur->fullCount);
+        if (bottomUp) {
+            if (!(found >= size || (double)found > (double)a.n / a.beta)) {
+                bottomUp = false;
+                scout = 1;
+            }
+        } else {
+            scout = nextE;
+        }
+        lastStrat = strat;
+        ++level;
+    }
+    // epilogue: depths of the (vertex, source) pairs never reached
+    for (uint64_t base = (uint64_t)blockIdx.x * NT; base < a.n; base += gthreads) {
+        const uint64_t v = base + tid;
+        const unsigned long long miss = v < a.n ? (a.all & ~a.seen[v]) : 0ull;
+        writeDepths(a, v, miss, kInf);
+    }
+    if (gtid == 0) {
+        if (a.trace && level > 0 && level - 1 < a.traceCap && lastStrat == GB_STRAT_BU)
+            a.trace[level - 1].edges = ldv64(&a.ctr[(level + 3) & 3].examined);
+        a.ctl[2] = level;
+    }
+}
+
+}  // namespace
+}  // namespace gb
+
+using namespace gb;
+
+void gb_bfs::ensureBatch(const gb_bfs_options& o, int k) {
+    const int block = o.block ? (int)o.block : 512;
+    const uint64_t hubCap = std::min<uint64_t>(n, m / 32 + 1);
+    bSeen.ensure(n);
+    bNext.ensure(n);
+    for (int i = 0; i < 2; ++i) {
+        bFront[i].ensure(n);
+        bActive[i].ensure(3 * n);  // vertex | start | degree
+        bHubV[i].ensure(2 * hubCap);  // vertex | start
+        bHubOff[i].ensure(hubCap);
+    }
+    bCand.ensure(n);
+    bDist.ensure((uint64_t)k * n + 4);
+    pctl.ensure(4);
+    ptrace.ensure(kTraceCap);
+    if (bBlock != block) {
+        int perSm = 0;
+        if (block == 256)
+            GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, batchBfsKernel<256>, 256, 0));
+        else
+            GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, batchBfsKernel<512>, 512, 0));
+        if (perSm < 1) throw Error(GB_ERR_CUDA, "batched BFS kernel cannot be resident");
+        bGrid = perSm * deviceSmCount();
+        bBlock = block;
+    }
+}
+
+void gb_bfs::runBatch(const uint32_t* src, int k, const gb_bfs_options& o, std::vector<gb_level>* tr) {
+    validateOptions(o);
+    if (k < 1 || k > 64) throw Error(GB_ERR_ARG, "batched BFS takes 1 to 64 sources");
+    for (int i = 0; i < k; ++i)
+        if (src[i] >= n) throw Error(GB_ERR_ARG, "source out of range");
+    if (o.selector == GB_SELECT_LEARNED && !selLoaded[1])
+        throw Error(GB_ERR_STATE, "learned batched selector requested but no parameters are loaded");
+    ensureBatch(o, k);
+    DevBuf<BCounters> ctr;
+    ctr.ensure(4);
+    DevBuf<uint32_t> dsrc;
+    dsrc.ensure(64);
+    hstage.ensure(64);
+    std::memcpy(hstage.p, src, k * 4);
+    GB_CUDA(cudaMemcpyAsync(dsrc.get(), hstage.p, k * 4, cudaMemcpyHostToDevice, stream.s));
+    BArgs a{};
+    a.row_ptr = rowPtr.get();
+    a.col_idx = colIdx.get();
+    a.seen = bSeen.get();
+    a.nx = bNext.get();
+    for (int i = 0; i < 2; ++i) {
+        a.fr[i] = bFront[i].get();
+        a.qv[i] = bActive[i].get();
+        a.qs[i] = bActive[i].get() + n;
+        a.qd[i] = bActive[i].get() + 2 * n;
+        const uint64_t hubCap = std::min<uint64_t>(n, m / 32 + 1);
+        a.hv[i] = bHubV[i].get();
+        a.hs[i] = bHubV[i].get() + hubCap;
+        a.ho[i] = bHubOff[i].get();
+    }
+    a.cq = bCand.get();
+    a.dist = bDist.get();
+    a.sources = dsrc.get();
+    a.ctr = ctr.get();
+    a.ctl = pctl.get();
+    a.trace = ptrace.get();
+    a.sel = selLoaded[1] ? selParams[1].get() : nullptr;
+    a.n = n;
+    a.m = m;
+    a.all = k == 64 ? ~0ull : ((1ull << k) - 1);
+    a.k = k;
+    a.hubMin = std::max<uint32_t>(o.hub_min, 32);
+    a.traceCap = kTraceCap;
+    a.alpha = o.alpha;
+    a.beta = o.beta;
+    a.selector = (int)o.selector;
+    a.force = o.force_strategy;
+    a.spinLimit = o.spin_limit ? o.spin_limit : (1ull << 24);
+    GB_CUDA(cudaMemsetAsync(pctl.get(), 0, 4 * sizeof(unsigned), stream.s));
+    GB_CUDA(cudaEventRecord(ev.a, stream.s));
+    void* args[] = {&a};
+    if (bBlock == 256)
+        GB_CUDA(cudaLaunchCooperativeKernel((void*)batchBfsKernel<256>, dim3(bGrid), dim3(256), args, 0, stream.s));
+    else
+        GB_CUDA(cudaLaunchCooperativeKernel((void*)batchBfsKernel<512>, dim3(bGrid), dim3(512), args, 0, stream.s));
+    GB_CUDA(cudaEventRecord(ev.b, stream.s));
+    unsigned ctl[4];
+    GB_CUDA(cudaMemcpyAsync(ctl, pctl.get(), sizeof ctl, cudaMemcpyDeviceToHost, stream.s));
+    GB_CUDA(cudaStreamSynchronize(stream.s));
+    lastGpuMs = ev.ms();
+    lastLevels = ctl[2];
+    if (ctl[1]) throw Error(GB_ERR_TIMEOUT, "batched BFS: grid barrier wait exceeded its spin limit");
+    if (tr) {
+        const uint32_t kk = std::min<uint32_t>(ctl[2], kTraceCap);
+        std::vector<gb_level> t(kk);
+        if (kk) GB_CUDA(cudaMemcpy(t.data(), ptrace.get(), kk * sizeof(gb_level), cudaMemcpyDeviceToHost));
+        for (auto& r : t) r.pad = 0;
+        tr->insert(tr->end(), t.begin(), t.end());
+    }
+}

@@ -21,6 +21,7 @@
 #include <cstring>
 
 #include "bfs.hpp"
+#include "bfs_device.cuh"
 
 namespace gb {
 namespace {
@@ -56,46 +57,6 @@ struct PArgs {
     uint32_t startLevel, maxLevels;
 };
 
-template <int NT>
-__device__ __forceinline__ uint32_t blockScan(uint32_t v, uint32_t* total, uint32_t* sm) {
-    constexpr int W = NT / 32;
-    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(kFull, x, o);
-        if ((int)lane >= o) x += y;
-    }
-    if (lane == 31) sm[wid] = x;
-    __syncthreads();
-    if (wid == 0) {
-        uint32_t w = lane < W ? sm[lane] : 0u, incl = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(kFull, incl, o);
-            if ((int)lane >= o) incl += y;
-        }
-        if (lane < W) sm[lane] = incl - w;
-        if (lane == W - 1) sm[W] = incl;
-    }
-    __syncthreads();
-    uint32_t r = sm[wid] + x - v;
-    *total = sm[W];
-    __syncthreads();
-    return r;
-}
-
-// Largest i in [lo, hi] with off[i] <= e.
-template <class T>
-__device__ __forceinline__ uint32_t ownerOf(const T* off, uint32_t lo, uint32_t hi, T e) {
-    while (lo < hi) {
-        uint32_t mid = (lo + hi + 1) >> 1;
-        if (off[mid] <= e) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 __device__ __forceinline__ unsigned long long ldv(const unsigned long long* p) {
     return *reinterpret_cast<const volatile unsigned long long*>(p);
 }
@@ -111,13 +72,16 @@ struct Acc {
 __device__ __forceinline__ void discover(const PArgs& a, bool has, uint32_t u, uint32_t level, GbPCounters* cur,
                                          uint32_t* bmNext, uint32_t nq, Acc& acc) {
     bool claimed = false;
-    uint32_t w = u >> 5, bit = 1u << (u & 31);
-    if (has && !(a.visited[w] & bit)) claimed = !(atomicOr(&a.visited[w], bit) & bit);
+    const uint32_t w = u >> 5, bit = 1u << (u & 31);
+    uint32_t st = 0, en = 0;
+    if (has && !(a.visited[w] & bit)) {
+        st = a.row_ptr[u];  // issued alongside the claim: no extra dependent step
+        en = a.row_ptr[u + 1];
+        claimed = !(atomicOr(&a.visited[w], bit) & bit);
+    }
     if (!__any_sync(kFull, claimed)) return;
-    uint32_t st = 0, d = 0;
+    const uint32_t d = claimed ? en - st : 0u;
     if (claimed) {
-        st = a.row_ptr[u];
-        d = a.row_ptr[u + 1] - st;
         a.dist[u] = level + 1;
         atomicOr(&bmNext[w], bit);
         acc.found++;
@@ -207,7 +171,8 @@ __device__ void tdWarpItem(const PArgs& a, uint32_t item, uint32_t S, uint32_t q
     }
 }
 
-// One chunk of the hubs' concatenated edge space, split over the block.
+// One chunk of the hubs' concatenated edge space, split over the block; two
+// edges per thread per round so their loads overlap.
 template <int NT>
 __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e1, uint32_t H, uint32_t qc,
                            uint32_t level, GbPCounters* cur, uint32_t* bmNext, Acc& acc) {
@@ -219,15 +184,21 @@ __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e
     }
     __syncthreads();
     const uint32_t lo = sm.range[0], hi = sm.range[1];
-    for (uint64_t base = e0; base < e1; base += NT) {
-        const uint64_t e = base + threadIdx.x;
-        const bool has = e < e1;
-        uint32_t u = 0;
-        if (has) {
-            const uint32_t o = ownerOf(ho, lo, hi, (unsigned long long)e);
-            u = a.col_idx[a.hs[qc][o] + (uint32_t)(e - ho[o])];
+    for (uint64_t base = e0; base < e1; base += 2 * NT) {
+        uint32_t u[2];
+        bool has[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint64_t e = base + k * NT + threadIdx.x;
+            has[k] = e < e1;
+            u[k] = 0;
+            if (has[k]) {
+                const uint32_t o = ownerOf(ho, lo, hi, (unsigned long long)e);
+                u[k] = a.col_idx[a.hs[qc][o] + (uint32_t)(e - ho[o])];
+            }
         }
-        discover(a, has, u, level, cur, bmNext, qc ^ 1u, acc);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) discover(a, has[k], u[k], level, cur, bmNext, qc ^ 1u, acc);
     }
     __syncthreads();
 }
@@ -250,16 +221,45 @@ __device__ void buLevel(const PArgs& a, uint32_t level, Acc& acc) {
         if (!((vw >> lane) & 1u)) {
             b = a.row_ptr[v];
             e = a.row_ptr[v + 1];
+            // First parent in the frontier, scanning in list order; aligned
+            // groups of 4 entries are loaded at once and their 4 frontier
+            // words fetched together, so a step costs two dependent loads
+            // for 4 entries.  `stop` is one past the first hit (or e).
+            uint32_t stop = e;
             uint32_t i = b;
-            for (; i < e; ++i) {
+            for (; i < e && (i & 3u); ++i) {
                 const uint32_t u = a.col_idx[i];
                 if ((front[u >> 5] >> (u & 31)) & 1u) {
+                    stop = i + 1;
                     found = true;
-                    ++i;
                     break;
                 }
             }
-            acc.exam += i - b;
+            if (!found) {
+                for (; i + 4 <= e; i += 4) {
+                    const uint4 q = *reinterpret_cast<const uint4*>(a.col_idx + i);
+                    const uint32_t f0 = front[q.x >> 5], f1 = front[q.y >> 5], f2 = front[q.z >> 5],
+                                   f3 = front[q.w >> 5];
+                    const unsigned hits = ((f0 >> (q.x & 31)) & 1u) | (((f1 >> (q.y & 31)) & 1u) << 1) |
+                                          (((f2 >> (q.z & 31)) & 1u) << 2) | (((f3 >> (q.w & 31)) & 1u) << 3);
+                    if (hits) {
+                        stop = i + __ffs(hits);
+                        found = true;
+                        break;
+                    }
+                }
+            }
+            if (!found) {
+                for (; i < e; ++i) {
+                    const uint32_t u = a.col_idx[i];
+                    if ((front[u >> 5] >> (u & 31)) & 1u) {
+                        stop = i + 1;
+                        found = true;
+                        break;
+                    }
+                }
+            }
+            acc.exam += stop - b;
         }
         const unsigned F = __ballot_sync(kFull, found);
         if (found) {
@@ -455,11 +455,12 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
             const uint64_t HE = hp & kHubMask;
             const uint32_t per = strat == GB_STRAT_TD_WARP ? NT / 32 : NT;
             const uint32_t nt = (S + per - 1) / per;
-            const uint64_t HC = (uint64_t)NT * 8;
+            const uint64_t HC = (uint64_t)NT * 2;
             const uint32_t nh = (uint32_t)((HE + HC - 1) / HC);
             uint32_t* bmNext = a.bm[(level + 1) % 3];
-            for (;;) {
-                if (tid == 0) sm.item = atomicAdd(&cur->work, 1u);
+            // block b takes item b first; further items come from a ticket
+            for (bool first = true;; first = false) {
+                if (tid == 0) sm.item = first ? blockIdx.x : gridDim.x + atomicAdd(&cur->work, 1u);
                 __syncthreads();
                 const uint32_t item = sm.item;
                 __syncthreads();

@@ -1,0 +1,776 @@
+// pagerank.cu -- PageRank on the GPU: push, scalar / vector / degree-adaptive
+// pull, in-place (Gauss-Seidel) sweeps and a double-precision pull oracle.
+//
+// Definition (src/cpu/pagerank_cpu.hpp:4-8): d = 0.85, r0 = 1/n,
+//   r_new[v] = (1-d)/n + d * (sum_{u in in(v)} r[u]/outdeg[u] + dangling/n).
+// Precision (FP32 ranks): per-vertex sums are Kahan-compensated (the star's
+// hub has 100k equal terms, src/shaders/pagerank.metal:27-42); the dangling
+// mass is a float-float (TwoSum) accumulation; the L1 residual and the
+// in-place renormalisation sum are FP64.  push uses compensated float atomics
+// (TwoSum error into a second accumulator, src/shaders/pagerank.metal:196-226).
+//
+// Structure (B200): one kernel per Jacobi iteration does the gather, the
+// store, the next iteration's contributions r/outdeg, the dangling mass and
+// (tol mode) the residual; its last block to finish (ticket on the control
+// block) reduces the per-block partials in a fixed order and advances the
+// iteration control on the device.  Iterations are therefore independent of
+// the host and replayed as CUDA graphs: fixed mode is one graph, tol mode
+// graphs of 8 iterations with one host check per batch (the reference
+// synchronises every iteration, src/metal/pagerank_gpu.mm:384-405).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "pagerank.hpp"
+
+namespace gb {
+namespace {
+
+constexpr int kMaxGrid = 4096;
+constexpr int kGraphBatch = 8;
+
+struct PrArgs {
+    const uint32_t* rp;
+    const uint32_t* ci;
+    const uint32_t* outdeg;
+    float* r[2];
+    float* contrib[2];
+    double* r64[2];
+    double* contrib64[2];
+    float* acc;
+    float* accLo;
+    const uint32_t* list;  // adaptive: list0|list1|list2; GS natural: the list to sweep
+    uint32_t cnt[3];
+    GbPrControl* ctl;
+    float* partF;
+    double* partD;
+    uint32_t n;
+    float damping, base, invN;
+    double base64, invN64, damping64;
+    uint32_t lo, hi;  // GS colored: id range of the set
+};
+
+struct Kahan {
+    float sum = 0.f, comp = 0.f;
+    __device__ __forceinline__ void add(float x) {
+        float y = x - comp;
+        float t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+    }
+};
+
+// float-float accumulator: (hi, lo) with |lo| << |hi|, combined by TwoSum.
+struct FF {
+    float hi = 0.f, lo = 0.f;
+    __device__ __forceinline__ void add(float x) {
+        float s = hi + x;
+        float bp = s - hi;
+        float err = (hi - (s - bp)) + (x - bp);
+        hi = s;
+        lo += err;
+    }
+    __device__ __forceinline__ void add(FF o) {
+        add(o.hi);
+        lo += o.lo;
+    }
+};
+
+__device__ __forceinline__ int ldvi(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+
+__device__ __forceinline__ float prValue(const PrArgs& a, float s, float dang) {
+    return a.base + a.damping * (s + dang * a.invN);  // pr_value, src/shaders/pagerank.metal:45-48
+}
+
+// Per-thread accumulators of one iteration.
+struct IterAcc {
+    FF dang;
+    double dsum = 0;
+    float dmax = 0;
+    double d64 = 0;
+};
+
+// Store of vertex v in a Jacobi iteration: r_new, the next contribution, the
+// dangling mass and the residual against the previous iterate.
+__device__ __forceinline__ void storeJacobi(const PrArgs& a, int cur, bool withDelta, uint32_t v, float val,
+                                            IterAcc& acc) {
+    a.r[cur ^ 1][v] = val;
+    const uint32_t od = a.outdeg[v];
+    a.contrib[cur ^ 1][v] = od ? val / (float)od : 0.0f;
+    if (!od) acc.dang.add(val);
+    if (withDelta) {
+        const float o = a.r[cur][v];
+        const double d = fabs((double)val - (double)o);
+        acc.dsum += d;
+        acc.dmax = fmaxf(acc.dmax, (float)d / fmaxf(val, a.invN));
+    }
+}
+
+// Block-wide reduction of IterAcc into thread 0 (fixed order: deterministic).
+__device__ __forceinline__ IterAcc blockReduceAcc(IterAcc acc) {
+    __shared__ float sHi[32], sLo[32], sMax[32];
+    __shared__ double sSum[32], s64[32];
+    const unsigned lane = laneId(), wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        FF other;
+        other.hi = __shfl_xor_sync(kFull, acc.dang.hi, o);
+        other.lo = __shfl_xor_sync(kFull, acc.dang.lo, o);
+        if (lane < (unsigned)o) acc.dang.add(other);  // lane 0 ends with the exact warp total
+        acc.dsum += __shfl_xor_sync(kFull, acc.dsum, o);
+        acc.d64 += __shfl_xor_sync(kFull, acc.d64, o);
+        acc.dmax = fmaxf(acc.dmax, __shfl_xor_sync(kFull, acc.dmax, o));
+    }
+    if (lane == 0) {
+        sHi[wid] = acc.dang.hi;
+        sLo[wid] = acc.dang.lo;
+        sSum[wid] = acc.dsum;
+        s64[wid] = acc.d64;
+        sMax[wid] = acc.dmax;
+    }
+    __syncthreads();
+    IterAcc t;
+    if (threadIdx.x == 0) {
+        for (unsigned w = 0; w < nw; ++w) {
+            FF x;
+            x.hi = sHi[w];
+            x.lo = sLo[w];
+            t.dang.add(x);
+            t.dsum += sSum[w];
+            t.d64 += s64[w];
+            t.dmax = fmaxf(t.dmax, sMax[w]);
+        }
+    }
+    __syncthreads();
+    return t;
+}
+
+// Each block writes its partials; the last block to finish (ticket on the
+// control block) reduces all partials in a fixed order and updates the
+// control block:
+//   kind 0: Jacobi iteration (dangling + residual + iteration advance)
+//   kind 1: contribution pass (dangling only)
+//   kind 2: renormalisation sum (sum64 only)
+//   kind 3: in-place scale (residual + iteration advance)
+//   kind 4: FP64 Jacobi iteration (dang64 + residual + advance)
+//   kind 5: FP64 initialisation (dang64 only)
+template <int KIND>
+__device__ void finishBlock(const PrArgs& a, IterAcc acc) {
+    __shared__ bool sLast;
+    IterAcc b = blockReduceAcc(acc);
+    if (threadIdx.x == 0) {
+        a.partF[2 * blockIdx.x] = b.dang.hi;
+        a.partF[2 * blockIdx.x + 1] = b.dang.lo;
+        a.partD[3 * blockIdx.x] = b.dsum;
+        a.partD[3 * blockIdx.x + 1] = b.d64;
+        a.partD[3 * blockIdx.x + 2] = b.dmax;
+        __threadfence();
+        sLast = atomicAdd(&a.ctl->done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!sLast) return;
+    __threadfence();
+    IterAcc p;
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+        FF x;
+        x.hi = __ldcg(&a.partF[2 * k]);
+        x.lo = __ldcg(&a.partF[2 * k + 1]);
+        p.dang.add(x);
+        p.dsum += __ldcg(&a.partD[3 * k]);
+        p.d64 += __ldcg(&a.partD[3 * k + 1]);
+        p.dmax = fmaxf(p.dmax, (float)__ldcg(&a.partD[3 * k + 2]));
+    }
+    IterAcc t = blockReduceAcc(p);
+    if (threadIdx.x != 0) return;
+    GbPrControl* c = a.ctl;
+    c->done = 0;
+    if (KIND == 0 || KIND == 1) {
+        c->dangHi = t.dang.hi;
+        c->dangLo = t.dang.lo;
+    }
+    if (KIND == 4 || KIND == 5) c->dang64 = t.d64;
+    if (KIND == 2) c->sum64 = t.dsum;
+    if (KIND == 0 || KIND == 3 || KIND == 4) {
+        c->iters += 1;
+        c->cur ^= 1;
+        if (c->withDelta) {
+            const double sum = t.dsum;
+            const float mx = t.dmax;
+            c->lastDelta = sum;
+            c->lastMaxRel = mx;
+            if (sum < c->tol && (c->tolRel <= 0 || mx < c->tolRel)) {
+                c->stopped = 1;
+            } else if (sum < c->best) {
+                c->best = sum;
+                c->sinceBest = 0;
+            } else if (++c->sinceBest >= 5) {
+                c->stopped = 1;
+                c->floorStop = 1;
+            }
+        }
+        if (c->iters >= c->cap) c->stopped = 1;
+    }
+}
+
+// r = 1/n, contrib = r/outdeg, dangling mass.
+__global__ void prInitKernel(PrArgs a) {
+    IterAcc acc;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < a.n; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = base + threadIdx.x;
+        if (v < a.n) {
+            a.r[0][v] = a.invN;
+            const uint32_t od = a.outdeg[v];
+            a.contrib[0][v] = od ? a.invN / (float)od : 0.0f;
+            if (!od) acc.dang.add(a.invN);
+        }
+    }
+    finishBlock<1>(a, acc);
+}
+
+__global__ void prInit64Kernel(PrArgs a) {
+    IterAcc acc;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < a.n; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = base + threadIdx.x;
+        if (v < a.n) {
+            a.r64[0][v] = a.invN64;
+            const uint32_t od = a.outdeg[v];
+            a.contrib64[0][v] = od ? a.invN64 / (double)od : 0.0;
+            if (!od) acc.d64 += a.invN64;
+        }
+    }
+    finishBlock<5>(a, acc);
+}
+
+// Kahan sum of contrib over v's in-list [b, e), lanes of a group of G threads
+// striding it; 16-byte aligned vector loads of col_idx (entries outside
+// [b, e) are masked; the array is padded so the last vector stays in bounds).
+template <bool COHERENT>
+__device__ __forceinline__ float ldContrib(const float* p) {
+    if (COHERENT) return *reinterpret_cast<const volatile float*>(p);  // rewritten during the sweep
+    return __ldg(p);
+}
+
+template <int G, bool COHERENT = false>
+__device__ __forceinline__ float gatherStrided(const uint32_t* __restrict__ ci, const float* contrib, uint32_t b,
+                                               uint32_t e, unsigned rank) {
+    Kahan k;
+    for (uint32_t i = (b & ~3u) + 4 * rank; i < e; i += 4 * G) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(ci + i));
+        if (i >= b) k.add(ldContrib<COHERENT>(contrib + q.x));
+        if (i + 1 >= b && i + 1 < e) k.add(ldContrib<COHERENT>(contrib + q.y));
+        if (i + 2 >= b && i + 2 < e) k.add(ldContrib<COHERENT>(contrib + q.z));
+        if (i + 3 >= b && i + 3 < e) k.add(ldContrib<COHERENT>(contrib + q.w));
+    }
+    return k.sum;
+}
+
+template <bool COHERENT = false>
+__device__ __forceinline__ float gatherSerial(const uint32_t* __restrict__ ci, const float* contrib, uint32_t b,
+                                              uint32_t e) {
+    Kahan k;
+    for (uint32_t i = b; i < e; ++i) k.add(ldContrib<COHERENT>(contrib + __ldg(ci + i)));
+    return k.sum;
+}
+
+__device__ __forceinline__ float blockSum(float x, float* sm) {
+    x = warpSum(x);
+    const unsigned lane = laneId(), wid = threadIdx.x >> 5;
+    if (lane == 0) sm[wid] = x;
+    __syncthreads();
+    float t = 0;
+    if (threadIdx.x == 0)
+        for (unsigned w = 0; w < (blockDim.x >> 5); ++w) t += sm[w];
+    __syncthreads();
+    return t;  // meaningful in thread 0
+}
+
+// Jacobi pull iteration.  MODE 0: thread per vertex (gpu_pull_scalar);
+// 1: warp per vertex (gpu_pull_vector); 2: degree-adaptive over the three
+// in-degree bins in one launch (block per large, warp per medium, thread per
+// small vertex; gpu_pull_adaptive).  INPLACE: the sweep of an in-place
+// variant -- contributions are read and rewritten in contrib[0] as vertices
+// are updated, and dangling / residual / control are left to the
+// contribution, sum and scale kernels.
+template <int MODE, bool INPLACE>
+__global__ void prPullKernel(PrArgs a) {
+    __shared__ float sRed[32];
+    const GbPrControl* c = a.ctl;
+    if (ldvi(&c->stopped)) return;
+    const int cur = c->cur;
+    const float dang = c->dangHi + c->dangLo;
+    const bool withDelta = !INPLACE && c->withDelta;
+    const float* contrib = INPLACE ? a.contrib[0] : a.contrib[cur];
+    IterAcc acc;
+    auto store = [&](uint32_t v, float s) {
+        const float val = prValue(a, s, dang);
+        if (INPLACE) {
+            a.r[cur ^ 1][v] = val;
+            const uint32_t od = a.outdeg[v];
+            a.contrib[0][v] = od ? val / (float)od : 0.0f;
+        } else {
+            storeJacobi(a, cur, withDelta, v, val, acc);
+        }
+    };
+    const uint64_t gthreads = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (MODE == 0) {
+        for (uint64_t v = gtid; v < a.n; v += gthreads)
+            store((uint32_t)v, gatherSerial<INPLACE>(a.ci, contrib, a.rp[v], a.rp[v + 1]));
+    } else if (MODE == 1) {
+        const uint64_t nwarps = gthreads >> 5;
+        for (uint64_t v = gtid >> 5; v < a.n; v += nwarps) {
+            float s = gatherStrided<32, INPLACE>(a.ci, contrib, a.rp[v], a.rp[v + 1], laneId());
+            s = warpSum(s);
+            if (laneId() == 0) store((uint32_t)v, s);
+        }
+    } else {
+        const uint32_t* l0 = a.list;
+        const uint32_t* l1 = l0 + a.cnt[0];
+        const uint32_t* l2 = l1 + a.cnt[1];
+        for (uint32_t i = blockIdx.x; i < a.cnt[2]; i += gridDim.x) {  // large: block per vertex
+            const uint32_t v = l2[i];
+            const uint32_t b = a.rp[v], e = a.rp[v + 1];
+            Kahan k;
+            for (uint32_t j = (b & ~3u) + 4 * threadIdx.x; j < e; j += 4 * blockDim.x) {
+                const uint4 q = __ldg(reinterpret_cast<const uint4*>(a.ci + j));
+                if (j >= b) k.add(ldContrib<INPLACE>(contrib + q.x));
+                if (j + 1 >= b && j + 1 < e) k.add(ldContrib<INPLACE>(contrib + q.y));
+                if (j + 2 >= b && j + 2 < e) k.add(ldContrib<INPLACE>(contrib + q.z));
+                if (j + 3 >= b && j + 3 < e) k.add(ldContrib<INPLACE>(contrib + q.w));
+            }
+            const float s = blockSum(k.sum, sRed);
+            if (threadIdx.x == 0) store(v, s);
+        }
+        const uint64_t nwarps = gthreads >> 5;
+        for (uint64_t i = gtid >> 5; i < a.cnt[1]; i += nwarps) {  // medium: warp per vertex
+            const uint32_t v = l1[i];
+            float s = gatherStrided<32, INPLACE>(a.ci, contrib, a.rp[v], a.rp[v + 1], laneId());
+            s = warpSum(s);
+            if (laneId() == 0) store(v, s);
+        }
+        for (uint64_t i = gtid; i < a.cnt[0]; i += gthreads) {  // small: thread per vertex
+            const uint32_t v = l0[i];
+            store(v, gatherSerial<INPLACE>(a.ci, contrib, a.rp[v], a.rp[v + 1]));
+        }
+    }
+    if (!INPLACE) finishBlock<0>(a, acc);
+}
+
+// In-place sweep over a vertex list, warp per vertex (natural GS order; the
+// deferred mutual-pair partners form a second list swept afterwards).
+__global__ void gsSweepListKernel(PrArgs a, uint32_t count) {
+    const GbPrControl* c = a.ctl;
+    if (ldvi(&c->stopped)) return;
+    const int cur = c->cur;
+    const float dang = c->dangHi + c->dangLo;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < count; i += nwarps) {
+        const uint32_t v = a.list[i];
+        Kahan k;
+        for (uint32_t j = a.rp[v] + laneId(); j < a.rp[v + 1]; j += 32)
+            k.add(*(volatile const float*)(a.contrib[0] + a.ci[j]));
+        const float s = warpSum(k.sum);
+        if (laneId() == 0) {
+            const float val = prValue(a, s, dang);
+            a.r[cur ^ 1][v] = val;
+            const uint32_t od = a.outdeg[v];
+            a.contrib[0][v] = od ? val / (float)od : 0.0f;
+        }
+    }
+}
+
+// In-place sweep of one colour set [lo, hi) of the relabeled graph, thread
+// per vertex (colored GS order).
+__global__ void gsSweepSetKernel(PrArgs a) {
+    const GbPrControl* c = a.ctl;
+    if (ldvi(&c->stopped)) return;
+    const int cur = c->cur;
+    const float dang = c->dangHi + c->dangLo;
+    for (uint64_t v = a.lo + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.hi;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        Kahan k;
+        for (uint32_t j = a.rp[v]; j < a.rp[v + 1]; ++j) k.add(*(volatile const float*)(a.contrib[0] + a.ci[j]));
+        const float val = prValue(a, k.sum, dang);
+        a.r[cur ^ 1][v] = val;
+        const uint32_t od = a.outdeg[v];
+        a.contrib[0][v] = od ? val / (float)od : 0.0f;
+    }
+}
+
+// In-place variants: contributions and dangling mass of the current iterate.
+__global__ void gsContribKernel(PrArgs a) {
+    const GbPrControl* c = a.ctl;
+    if (ldvi(&c->stopped)) return;
+    const int cur = c->cur;
+    IterAcc acc;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < a.n; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = base + threadIdx.x;
+        if (v < a.n) {
+            const float r = a.r[cur][v];
+            const uint32_t od = a.outdeg[v];
+            a.contrib[0][v] = od ? r / (float)od : 0.0f;
+            if (!od) acc.dang.add(r);
+        }
+    }
+    finishBlock<1>(a, acc);
+}
+
+// FP64 sum of the new iterate (renormalisation, src/shaders/pagerank.metal:86-117).
+__global__ void prSumKernel(PrArgs a) {
+    const GbPrControl* c = a.ctl;
+    if (ldvi(&c->stopped)) return;
+    const float* rn = a.r[c->cur ^ 1];
+    IterAcc acc;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.n; v += (uint64_t)gridDim.x * blockDim.x)
+        acc.dsum += (double)rn[v];
+    finishBlock<2>(a, acc);
+}
+
+// Scale the new iterate to sum 1 (FP64 division), residual, advance.
+__global__ void prScaleKernel(PrArgs a) {
+    const GbPrControl* c = a.ctl;
+    if (ldvi(&c->stopped)) return;
+    const int cur = c->cur;
+    const double sum = c->sum64;
+    const bool withDelta = c->withDelta;
+    IterAcc acc;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < a.n; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = base + threadIdx.x;
+        if (v < a.n) {
+            const float val = (float)((double)a.r[cur ^ 1][v] / sum);
+            a.r[cur ^ 1][v] = val;
+            if (withDelta) {
+                const float o = a.r[cur][v];
+                const double d = fabs((double)val - (double)o);
+                acc.dsum += d;
+                acc.dmax = fmaxf(acc.dmax, (float)d / fmaxf(val, a.invN));
+            }
+        }
+    }
+    finishBlock<3>(a, acc);
+}
+
+// gpu_push: thread per source vertex scatters its contribution with float
+// atomics.  When every active lane of a warp targets the same vertex (a hub's
+// in-neighbours), the lanes sum first and issue one atomic.  Each atomic's
+// rounding error is recovered exactly by TwoSum against the returned old
+// value and, when it exceeds 2^-16 of the term, added to a second
+// accumulator (src/shaders/pagerank.metal:196-226).
+__device__ __forceinline__ void addCompensated(float* acc, float* accLo, uint32_t t, float x) {
+    const float old = atomicAdd(&acc[t], x);
+    const float s = old + x;
+    const float bp = s - old;
+    const float err = (old - (s - bp)) + (x - bp);
+    if (fabsf(err) > fabsf(x) * 0x1p-16f) atomicAdd(&accLo[t], err);
+}
+
+__global__ void prPushKernel(PrArgs a, const uint32_t* __restrict__ rowOut, const uint32_t* __restrict__ colOut) {
+    const GbPrControl* c = a.ctl;
+    if (ldvi(&c->stopped)) return;
+    const float* contrib = a.contrib[c->cur];
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < a.n; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t u = base + threadIdx.x;
+        const bool active = u < a.n;
+        const float cu = active ? contrib[u] : 0.0f;
+        const uint32_t b = active ? rowOut[u] : 0u;
+        const uint32_t deg = (active && cu != 0.0f) ? rowOut[u + 1] - b : 0u;
+        const uint32_t rounds = __reduce_max_sync(kFull, deg);
+        for (uint32_t k = 0; k < rounds; ++k) {
+            const bool has = k < deg;
+            const uint32_t t = has ? colOut[b + k] : 0xFFFFFFFFu;
+            const uint32_t lead = __reduce_min_sync(kFull, t);
+            if (__all_sync(kFull, !has || t == lead)) {
+                const float s = warpSum(has ? cu : 0.0f);
+                if (laneId() == 0) addCompensated(a.acc, a.accLo, lead, s);
+            } else if (has) {
+                addCompensated(a.acc, a.accLo, t, cu);
+            }
+        }
+    }
+}
+
+__global__ void prPushFinalizeKernel(PrArgs a) {
+    const GbPrControl* c = a.ctl;
+    if (ldvi(&c->stopped)) return;
+    const int cur = c->cur;
+    const float dang = c->dangHi + c->dangLo;
+    const bool withDelta = c->withDelta;
+    IterAcc acc;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < a.n; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = base + threadIdx.x;
+        if (v < a.n) {
+            const float val = prValue(a, a.acc[v] + a.accLo[v], dang);
+            a.acc[v] = 0.0f;
+            a.accLo[v] = 0.0f;
+            storeJacobi(a, cur, withDelta, (uint32_t)v, val, acc);
+        }
+    }
+    finishBlock<0>(a, acc);
+}
+
+// Double-precision Jacobi pull (warp per vertex): the GPU oracle against
+// which FP32 runs are measured at sizes where the CPU reference is slow.
+__global__ void prPullF64Kernel(PrArgs a) {
+    const GbPrControl* c = a.ctl;
+    if (ldvi(&c->stopped)) return;
+    const int cur = c->cur;
+    const double add = a.base64 + a.damping64 * c->dang64 * a.invN64;
+    const bool withDelta = c->withDelta;
+    const double* contrib = a.contrib64[cur];
+    IterAcc acc;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < a.n; v += nwarps) {
+        double s = 0;
+        for (uint32_t j = a.rp[v] + laneId(); j < a.rp[v + 1]; j += 32) s += contrib[a.ci[j]];
+        s = warpSum(s);
+        if (laneId() == 0) {
+            const double val = add + a.damping64 * s;
+            a.r64[cur ^ 1][v] = val;
+            const uint32_t od = a.outdeg[v];
+            a.contrib64[cur ^ 1][v] = od ? val / od : 0.0;
+            if (!od) acc.d64 += val;
+            if (withDelta) {
+                const double d = fabs(val - a.r64[cur][v]);
+                acc.dsum += d;
+                acc.dmax = fmaxf(acc.dmax, (float)(d / fmax(val, a.invN64)));
+            }
+        }
+    }
+    finishBlock<4>(a, acc);
+}
+
+}  // namespace
+}  // namespace gb
+
+using namespace gb;
+
+gb_pr::~gb_pr() { invalidateGraphs(); }
+
+// Cached graphs hold buffer addresses: drop them whenever a buffer they may
+// reference is (re)allocated.
+void gb_pr::invalidateGraphs() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
+}
+
+namespace {
+
+PrArgs makeArgs(gb_pr& h, bool relabeled) {
+    PrArgs a{};
+    a.rp = relabeled ? h.rowGS.get() : h.rowIn.get();
+    a.ci = relabeled ? h.colGS.get() : h.colIn.get();
+    a.outdeg = relabeled ? h.outdegGS.get() : h.outdeg.get();
+    for (int i = 0; i < 2; ++i) {
+        a.r[i] = h.r[i].get();
+        a.contrib[i] = h.contrib[i].get();
+        a.r64[i] = h.r64[i].get();
+        a.contrib64[i] = h.contrib64[i].get();
+    }
+    a.acc = h.acc.get();
+    a.accLo = h.accLo.get();
+    a.list = h.bins.get();
+    for (int i = 0; i < 3; ++i) a.cnt[i] = h.binCount[i];
+    a.ctl = h.ctl.get();
+    a.partF = h.partF.get();
+    a.partD = h.partD.get();
+    a.n = (uint32_t)h.n;
+    return a;
+}
+
+uint32_t gridFor(uint64_t work, uint32_t threads) {
+    uint64_t b = (work + threads - 1) / threads;
+    uint64_t cap = std::min<uint64_t>(kMaxGrid, (uint64_t)deviceSmCount() * (2048 / threads));
+    return (uint32_t)std::max<uint64_t>(1, std::min(b, cap));
+}
+
+}  // namespace
+
+// Enqueue one iteration of `variant` on the handle's stream (capturable).
+static void enqueueIteration(gb_pr& h, int v, const gb_pr_options& o, PrArgs& a, PrArgs& ag) {
+    const uint32_t tg = o.tg;
+    cudaStream_t s = h.stream.s;
+    const uint32_t gN = gridFor(h.n, 256);
+    auto pullGrid = [&](int mode) {
+        if (mode == 0) return gridFor(h.n, tg);
+        if (mode == 1) return gridFor(h.n * 32, tg);
+        return gridFor(std::max<uint64_t>({(uint64_t)h.binCount[0], (uint64_t)h.binCount[1] * 32,
+                                           (uint64_t)h.binCount[2] * tg}), tg);
+    };
+    const bool inplace = v == GB_PR_PULL_GS || (o.inplace && v != GB_PR_PUSH && v != GB_PR_PULL_F64);
+    if (v == GB_PR_PUSH) {
+        prPushKernel<<<gridFor(h.n, tg), tg, 0, s>>>(a, h.rowOut.get(), h.colOut.get());
+        prPushFinalizeKernel<<<gN, 256, 0, s>>>(a);
+    } else if (v == GB_PR_PULL_F64) {
+        prPullF64Kernel<<<gridFor(h.n * 32, tg), tg, 0, s>>>(a);
+    } else if (!inplace) {
+        if (v == GB_PR_PULL_SCALAR) prPullKernel<0, false><<<pullGrid(0), tg, 0, s>>>(a);
+        else if (v == GB_PR_PULL_VECTOR) prPullKernel<1, false><<<pullGrid(1), tg, 0, s>>>(a);
+        else prPullKernel<2, false><<<pullGrid(2), tg, 0, s>>>(a);
+    } else {
+        const bool colored = v == GB_PR_PULL_GS && h.gsColored;
+        PrArgs& w = colored ? ag : a;
+        gsContribKernel<<<gN, 256, 0, s>>>(w);
+        if (v == GB_PR_PULL_GS) {
+            if (colored) {
+                for (size_t k = 0; k + 1 < h.gsSetStart.size(); ++k) {
+                    PrArgs ws = w;
+                    ws.lo = h.gsSetStart[k];
+                    ws.hi = h.gsSetStart[k + 1];
+                    gsSweepSetKernel<<<gridFor(ws.hi - ws.lo, tg), tg, 0, s>>>(ws);
+                }
+            } else if (h.gsNatB > 0) {
+                PrArgs wa = w;
+                wa.list = h.gsNat.get();
+                gsSweepListKernel<<<gridFor((uint64_t)h.gsNatA * 32, tg), tg, 0, s>>>(wa, h.gsNatA);
+                wa.list = h.gsNat.get() + h.gsNatA;
+                gsSweepListKernel<<<gridFor((uint64_t)h.gsNatB * 32, tg), tg, 0, s>>>(wa, h.gsNatB);
+            } else {
+                prPullKernel<1, true><<<pullGrid(1), tg, 0, s>>>(w);
+            }
+        } else if (v == GB_PR_PULL_SCALAR) {
+            prPullKernel<0, true><<<pullGrid(0), tg, 0, s>>>(w);
+        } else if (v == GB_PR_PULL_VECTOR) {
+            prPullKernel<1, true><<<pullGrid(1), tg, 0, s>>>(w);
+        } else {
+            prPullKernel<2, true><<<pullGrid(2), tg, 0, s>>>(w);
+        }
+        prSumKernel<<<gN, 256, 0, s>>>(w);
+        prScaleKernel<<<gN, 256, 0, s>>>(w);
+    }
+    GB_LAUNCH_CHECK();
+}
+
+gb_pr_result gb_pr::run(int v, const gb_pr_options& o) {
+    if (o.tg < 32 || o.tg > 1024 || o.tg % 32)
+        throw Error(GB_ERR_ARG, "threadgroup size must be a multiple of 32 in [32, 1024]");
+    if (v < GB_PR_PUSH || v > GB_PR_PULL_F64) throw Error(GB_ERR_ARG, "unknown GPU PageRank variant");
+    if (v == GB_PR_PUSH && !hasOut) throw Error(GB_ERR_ARG, "gpu_push needs the out-CSR");
+    if (v != GB_PR_PUSH && !hasIn) throw Error(GB_ERR_ARG, "pull variants need the in-CSR");
+    if (o.iters < 0) throw Error(GB_ERR_ARG, "iters must be >= 0");
+    if (v == GB_PR_PULL_ADAPTIVE) prepareAdaptive(o.small_max, o.large_min);
+    if (v == GB_PR_PULL_GS && !gsReady) prepareGS(2);
+    gb_pr_result res{};
+    res.last_delta = -1;
+    res.last_max_rel = -1;
+    gsLastRun = v == GB_PR_PULL_GS && gsColored;
+    lastVariant = v;
+    if (n == 0) return res;
+    const void* before[6] = {r64[0].get(), r64[1].get(), contrib64[0].get(), contrib64[1].get(), acc.get(),
+                             accLo.get()};
+    if (v == GB_PR_PULL_F64) {
+        for (auto& b : r64) b.ensure(n);
+        for (auto& b : contrib64) b.ensure(n);
+    }
+    if (v == GB_PR_PUSH) {
+        acc.ensure(n);
+        accLo.ensure(n);
+    }
+    const void* after[6] = {r64[0].get(), r64[1].get(), contrib64[0].get(), contrib64[1].get(), acc.get(),
+                            accLo.get()};
+    if (std::memcmp(before, after, sizeof before) != 0) invalidateGraphs();
+    const bool tolMode = o.tol > 0;
+    GbPrControl c{};
+    c.cap = o.iters;
+    c.stopped = o.iters == 0;
+    c.withDelta = tolMode ? 1 : 0;
+    c.best = 1e300;
+    c.tol = o.tol;
+    c.tolRel = o.tol_rel;
+    PrArgs a = makeArgs(*this, false);
+    a.damping = o.damping;
+    a.base = (1.0f - o.damping) / (float)n;
+    a.invN = 1.0f / (float)n;
+    // The FP64 variant uses the decimal value the float option was written as
+    // (0.85f -> 0.85), as the double-precision CPU reference does.
+    {
+        char buf[32];
+        std::snprintf(buf, sizeof buf, "%.7g", (double)o.damping);
+        a.damping64 = std::strtod(buf, nullptr);
+    }
+    a.base64 = (1.0 - a.damping64) / (double)n;
+    a.invN64 = 1.0 / (double)n;
+    PrArgs ag = a;
+    if (gsColored && gsReady) {
+        ag.rp = rowGS.get();
+        ag.ci = colGS.get();
+        ag.outdeg = outdegGS.get();
+    }
+    const bool relabel = v == GB_PR_PULL_GS && gsColored;
+    GB_CUDA(cudaEventRecord(ev.a, stream.s));
+    GB_CUDA(cudaMemcpyAsync(ctl.get(), &c, sizeof c, cudaMemcpyHostToDevice, stream.s));
+    if (v == GB_PR_PUSH) {
+        GB_CUDA(cudaMemsetAsync(acc.get(), 0, n * 4, stream.s));
+        GB_CUDA(cudaMemsetAsync(accLo.get(), 0, n * 4, stream.s));
+    }
+    {
+        PrArgs ai = relabel ? ag : a;
+        if (v == GB_PR_PULL_F64) prInit64Kernel<<<gridFor(n, 256), 256, 0, stream.s>>>(ai);
+        else prInitKernel<<<gridFor(n, 256), 256, 0, stream.s>>>(ai);
+        GB_LAUNCH_CHECK();
+    }
+    // Iteration batches as CUDA graphs (cached per variant / shape).
+    const int batch = tolMode ? kGraphBatch : std::max(1, o.iters);
+    auto key = std::make_tuple(v, batch, (int)o.tg, (int)(o.inplace != 0), relabel ? 1 : 0, (int)binSmall,
+                               (int)binLarge);
+    cudaGraphExec_t exec = nullptr;
+    auto it = graphs.find(key);
+    if (it != graphs.end()) {
+        exec = it->second;
+    } else {
+        cudaGraph_t g;
+        GB_CUDA(cudaStreamBeginCapture(stream.s, cudaStreamCaptureModeThreadLocal));
+        try {
+            for (int i = 0; i < batch; ++i) enqueueIteration(*this, v, o, a, ag);
+        } catch (...) {
+            cudaStreamEndCapture(stream.s, &g);
+            throw;
+        }
+        GB_CUDA(cudaStreamEndCapture(stream.s, &g));
+        GB_CUDA(cudaGraphInstantiate(&exec, g, 0));
+        cudaGraphDestroy(g);
+        graphs[key] = exec;
+    }
+    GbPrControl hc{};
+    for (int launched = 0;;) {
+        GB_CUDA(cudaGraphLaunch(exec, stream.s));
+        launched += batch;
+        if (!tolMode) break;
+        GB_CUDA(cudaMemcpyAsync(&hc, ctl.get(), sizeof hc, cudaMemcpyDeviceToHost, stream.s));
+        GB_CUDA(cudaStreamSynchronize(stream.s));
+        if (hc.stopped || launched >= o.iters) break;
+    }
+    GB_CUDA(cudaEventRecord(ev.b, stream.s));
+    GB_CUDA(cudaMemcpyAsync(&hc, ctl.get(), sizeof hc, cudaMemcpyDeviceToHost, stream.s));
+    GB_CUDA(cudaStreamSynchronize(stream.s));
+    res.gpu_ms = ev.ms();
+    res.iters = hc.iters;
+    res.floor_stop = hc.floorStop;
+    if (tolMode) {
+        res.last_delta = hc.lastDelta;
+        res.last_max_rel = hc.lastMaxRel;
+    }
+    return res;
+}
+
+void gb_pr::ranks(float* out) {
+    if (lastVariant < 0) throw Error(GB_ERR_STATE, "ranks() before run()");
+    if (lastVariant == GB_PR_PULL_F64) throw Error(GB_ERR_STATE, "last run was FP64: use the double ranks");
+    GbPrControl hc{};
+    GB_CUDA(cudaMemcpy(&hc, ctl.get(), sizeof hc, cudaMemcpyDeviceToHost));
+    if (!gsLastRun) {
+        GB_CUDA(cudaMemcpy(out, r[hc.cur].get(), n * 4, cudaMemcpyDeviceToHost));
+        return;
+    }
+    std::vector<float> tmp(n);
+    GB_CUDA(cudaMemcpy(tmp.data(), r[hc.cur].get(), n * 4, cudaMemcpyDeviceToHost));
+    for (uint64_t v = 0; v < n; ++v) out[v] = tmp[gsNewId[v]];
+}
+
+void gb_pr::ranks64(double* out) {
+    if (lastVariant != GB_PR_PULL_F64) throw Error(GB_ERR_STATE, "no FP64 run to read");
+    GbPrControl hc{};
+    GB_CUDA(cudaMemcpy(&hc, ctl.get(), sizeof hc, cudaMemcpyDeviceToHost));
+    GB_CUDA(cudaMemcpy(out, r64[hc.cur].get(), n * 8, cudaMemcpyDeviceToHost));
+}

@@ -101,8 +101,9 @@ typedef enum {
     GB_BFS_BINNED = 2,     /* gpu_binned: runBinned, bfs_gpu.mm:177-236 */
     GB_BFS_EDGE = 3,       /* gpu_edge:   runEdge,   bfs_gpu.mm:277-305 */
     GB_BFS_DO = 4,         /* gpu_do:     runDO (host loop, one sync per level), bfs_gpu.mm:326-429 */
-    GB_BFS_PERSISTENT = 5  /* gpu_do_persistent: every level in one cooperative launch;
+    GB_BFS_PERSISTENT = 5, /* gpu_do_persistent: every level in one cooperative launch;
                               also what `hybrid` (bfs_gpu.mm:307-325) maps to */
+    GB_BFS_BATCH = 6       /* the 64-source batched kernel (gb_bfs_run_batch; autotune only) */
 } gb_bfs_variant;
 
 typedef enum { GB_SELECT_RULE = 0, GB_SELECT_LEARNED = 1 } gb_selector;
@@ -194,8 +195,10 @@ int gb_bfs_profile_batch_levels(gb_bfs* h, const uint32_t* sources, int k, const
                                 int repeats, float* feats_out, float* times_out, size_t cap,
                                 size_t* rows);
 
-/* Autotuner: pick small_max/large_min, ept, tg (and the persistent block size)
- * per graph by timing candidates on the given sources; writes the best into *o. */
+/* Autotuner (replaces scripts/sweep_balanced.sh, sweep_tg.sh, sweep_do.sh):
+ * times candidate small_max/large_min and tg (gpu_binned), ept and tg
+ * (gpu_edge, gpu_do), block size and hub_min cut (persistent, GB_BFS_BATCH)
+ * on the given sources and writes the fastest into *o. */
 int gb_bfs_autotune(gb_bfs* h, int variant, const uint32_t* sources, int k, gb_bfs_options* o);
 
 /* --------------------------------------------------------------- PageRank */

@@ -1,0 +1,61 @@
+"""64-source batched BFS (one launch, per-vertex 64-bit masks) against the
+oracle: every source's depths must equal cpu_serial's, whatever strategy runs
+each level and whatever the batch size, including repeated sources."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def check_batch(gb, oracle, g, bfs, srcs, opts):
+    d = bfs.run_batch(srcs, opts=opts)
+    for i, s in enumerate(srcs):
+        ref = oracle.bfs_serial(g, int(s))
+        assert np.array_equal(d[i], ref), (i, int(s))
+    return d
+
+
+def test_batch_suite_all_strategies(gb, oracle):
+    for name, g0 in gb.gen.suite():
+        g = gb.symmetrize(g0)
+        bfs = gb.GpuBfs(g)
+        rng = np.random.default_rng(len(name))
+        srcs = rng.integers(0, g.n, 64).astype(np.uint32)
+        refs = [oracle.bfs_serial(g, int(s)) for s in srcs]
+        for opts in [gb.BfsOptions()] + [gb.BfsOptions(force_strategy=s) for s in range(5)] + \
+                    [gb.BfsOptions(alpha=2.0, beta=2.0), gb.BfsOptions(hub_min=32, block=256)]:
+            d, tr = bfs.run_batch(srcs, opts=opts, trace=True)
+            for i in range(len(srcs)):
+                assert np.array_equal(d[i], refs[i]), (name, i, opts.force_strategy)
+
+
+def test_batch_sizes_and_duplicates(gb, oracle):
+    g = gb.gen.rmat(14, 16, False, 5)
+    bfs = gb.GpuBfs(g)
+    for srcs in ([3], [3, 3, 3], list(range(7)), [0] * 64, list(gb.pick_sources(g, 64, 2))):
+        check_batch(gb, oracle, g, bfs, np.array(srcs, np.uint32), gb.BfsOptions())
+    with pytest.raises(gb.GraphError):
+        bfs.run_batch(np.arange(65, dtype=np.uint32))
+    with pytest.raises(gb.GraphError):
+        bfs.run_batch(np.array([g.n], np.uint32))
+
+
+def test_batch_larger_graphs(gb, oracle):
+    graphs = [gb.gen.road(200, 200, 0.04, 0.005, 1), gb.gen.chung_lu(100000, 2.2, 30.0, 2),
+              gb.permute(gb.gen.rmat(17, 16, False, 3), gb.random_perm(1 << 17, 4))]
+    for g in graphs:
+        bfs = gb.GpuBfs(g)
+        srcs = gb.pick_sources(g, 64, 9)
+        for opts in (gb.BfsOptions(), gb.BfsOptions(force_strategy="bu"), gb.BfsOptions(force_strategy="td_ept2"),
+                     gb.BfsOptions(hub_min=64)):
+            check_batch(gb, oracle, g, bfs, srcs, opts)
+
+
+def test_batch_learned_selector_exact(gb, oracle):
+    g = gb.gen.rmat(15, 16, False, 8)
+    bfs = gb.GpuBfs(g)
+    srcs = gb.pick_sources(g, 64, 3)
+    rng = np.random.default_rng(5)
+    for _ in range(3):
+        bfs.set_selector(rng.normal(0, 1, gb.selector_param_count()).astype(np.float32), 1)
+        check_batch(gb, oracle, g, bfs, srcs, gb.BfsOptions(selector="learned"))
