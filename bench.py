@@ -246,9 +246,10 @@ def bfs_config_workload(args, world, rank, local):
     if sel2 is not None:
         bfs.set_selector(sel2, 1)
     o1 = G.BfsOptions(selector="learned" if sel1 is not None else "rule")
+    o1 = bfs.autotune("gpu_do_persistent", srcs64[:2], o1)
     ob = G.BfsOptions(selector="learned" if sel2 is not None else "rule")
     tuned = bfs.autotune("batch", srcs64, G.BfsOptions(selector=ob.selector))
-    ob.block, ob.hub_min = tuned.block, tuned.hub_min
+    ob.block, ob.hub_min, ob.grid_blocks = tuned.block, tuned.hub_min, tuned.grid_blocks
     # exactness of the batch against single-source runs (size-independent)
     d64 = bfs.run_batch(srcs64, opts=ob)
     for i in (0, 17, 63):
@@ -288,7 +289,9 @@ def bfs_config_workload(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": batch_t, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64 masks / u32 depths", "data": "synthetic",
             "config": {"workload": args.workload, "n": g.n, "m": g.m, "sources": 64, "batch_selector": ob.selector,
-                       "tuned_block": ob.block, "tuned_hub_min": ob.hub_min, "parallelism": f"replicas{world}"},
+                       "tuned_block": ob.block, "tuned_hub_min": ob.hub_min, "tuned_grid_blocks": ob.grid_blocks,
+                       "single_tuned": {"block": o1.block, "grid_blocks": o1.grid_blocks, "hub_min": o1.hub_min},
+                       "parallelism": f"replicas{world}"},
             "e2e": {"value": e64 / (e2e * 1e-3) / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 256,
                     "d2h_bytes_per_step": 4 * 64 * g.n},
             "gpu_launches": args.steps,
@@ -486,6 +489,8 @@ def main():
         bfs.set_selector(sel, 0)
         selector = "learned"
     opts = G.BfsOptions(selector=selector)
+    # per-graph autotuning of block size, grid size and hub cut (untimed)
+    opts = bfs.autotune("gpu_do_persistent", srcs[:4], opts)
     stream = torch.cuda.ExternalStream(G.lib().gb_bfs_stream(bfs._h))
 
     # exactness of one result (size-independent check) and TEPS denominators
@@ -581,6 +586,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": WORKLOAD if args.scale == SCALE else f"rmat{args.scale}_bfs{len(srcs)}", "n": g.n, "m": g.m, "sources": len(srcs), "selector": selector,
+                   "tuned": {"block": opts.block, "grid_blocks": opts.grid_blocks, "hub_min": opts.hub_min},
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (CSR 293 MB)",
                    "edges_per_step": edges_per_step},
         "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),

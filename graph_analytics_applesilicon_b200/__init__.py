@@ -49,7 +49,8 @@ class BfsOptions(C.Structure):
     _fields_ = [("tg", C.c_uint32), ("small_max", C.c_uint32), ("large_min", C.c_uint32),
                 ("ept", C.c_uint32), ("alpha", C.c_double), ("beta", C.c_double),
                 ("selector", C.c_uint32), ("force_strategy", C.c_int32), ("hub_min", C.c_uint32),
-                ("block", C.c_uint32), ("spin_limit", C.c_uint64)]
+                ("block", C.c_uint32), ("spin_limit", C.c_uint64), ("grid_blocks", C.c_uint32),
+                ("pad_", C.c_uint32)]
 
     def __init__(self, **kw):
         super().__init__()

@@ -53,14 +53,14 @@ struct gb_bfs {
     gb::DevBuf<unsigned> pctl;           // [0] barrier, [1] error, [2] levels, [3] flags
     gb::DevBuf<gb_level> ptrace;
     gb::DevBuf<double> pstate;           // level state for resumable (profiling) runs
-    int pGrid = 0, pBlock = 0;
+    int pGrid = 0, pBlock = 0, pMax = 0, pWant = 0;
 
     // batched (64 sources)
     gb::DevBuf<unsigned long long> bSeen, bFront[2], bNext;
     gb::DevBuf<uint32_t> bActive[2], bCand, bHubV[2];
     gb::DevBuf<unsigned long long> bHubOff[2];
     gb::DevBuf<uint32_t> bDist;          // k * n results
-    int bGrid = 0, bBlock = 0;
+    int bGrid = 0, bBlock = 0, bMax = 0;
 
     // learned selector parameters (single-source, batched)
     gb::DevBuf<float> selParams[2];

@@ -521,9 +521,10 @@ void gb_bfs::ensureBatch(const gb_bfs_options& o, int k) {
         else
             GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, batchBfsKernel<512>, 512, 0));
         if (perSm < 1) throw Error(GB_ERR_CUDA, "batched BFS kernel cannot be resident");
-        bGrid = perSm * deviceSmCount();
+        bMax = perSm * deviceSmCount();
         bBlock = block;
     }
+    bGrid = o.grid_blocks > 0 ? std::min<int>((int)o.grid_blocks, bMax) : bMax;
 }
 
 void gb_bfs::runBatch(const uint32_t* src, int k, const gb_bfs_options& o, std::vector<gb_level>* tr) {

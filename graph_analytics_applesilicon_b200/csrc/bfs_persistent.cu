@@ -70,11 +70,13 @@ struct Acc {
 // Claim u for level+1 (all 32 lanes call together) and append it to the next
 // frontier: bitmap bit, queue entry (degree < hub_min) or hub entry.
 __device__ __forceinline__ void discover(const PArgs& a, bool has, uint32_t u, uint32_t level, GbPCounters* cur,
-                                         uint32_t* bmNext, uint32_t nq, Acc& acc) {
+                                         uint32_t* bmNext, uint32_t nq, Acc& acc, bool precheck) {
     bool claimed = false;
     const uint32_t w = u >> 5, bit = 1u << (u & 31);
     uint32_t st = 0, en = 0;
-    if (has && !(a.visited[w] & bit)) {
+    // Small levels claim directly (one dependent round trip less); large ones
+    // read the visited word first to spare atomics on visited neighbours.
+    if (has && (!precheck || !(a.visited[w] & bit))) {
         st = a.row_ptr[u];  // issued alongside the claim: no extra dependent step
         en = a.row_ptr[u + 1];
         claimed = !(atomicOr(&a.visited[w], bit) & bit);
@@ -125,7 +127,7 @@ struct Smem {
 // binary search over the staged offsets.
 template <int NT, int EPT>
 __device__ void tdTile(const PArgs& a, Smem<NT>& sm, uint32_t item, uint32_t S, uint32_t qc, uint32_t level,
-                       GbPCounters* cur, uint32_t* bmNext, Acc& acc) {
+                       GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre) {
     const uint32_t idx = item * NT + threadIdx.x;
     uint32_t st = 0, d = 0;
     if (idx < S) {
@@ -152,22 +154,19 @@ __device__ void tdTile(const PArgs& a, Smem<NT>& sm, uint32_t item, uint32_t S, 
             }
         }
 #pragma unroll
-        for (int k = 0; k < EPT; ++k) discover(a, has[k], u[k], level, cur, bmNext, qc ^ 1u, acc);
+        for (int k = 0; k < EPT; ++k) discover(a, has[k], u[k], level, cur, bmNext, qc ^ 1u, acc, pre);
     }
     __syncthreads();
 }
 
 // Warp per queue entry (degree-binned form): lanes stride the adjacency list.
-template <int NT>
-__device__ void tdWarpItem(const PArgs& a, uint32_t item, uint32_t S, uint32_t qc, uint32_t level, GbPCounters* cur,
-                           uint32_t* bmNext, Acc& acc) {
-    const uint32_t idx = item * (NT / 32) + (threadIdx.x >> 5);
-    if (idx >= S) return;  // warp-uniform
+__device__ __forceinline__ void tdWarpEntry(const PArgs& a, uint32_t idx, uint32_t qc, uint32_t level,
+                                            GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre) {
     const uint32_t st = a.qs[qc][idx], d = a.qd[qc][idx];
     for (uint32_t base = 0; base < d; base += 32) {
         const uint32_t e = base + laneId();
         const bool has = e < d;
-        discover(a, has, has ? a.col_idx[st + e] : 0u, level, cur, bmNext, qc ^ 1u, acc);
+        discover(a, has, has ? a.col_idx[st + e] : 0u, level, cur, bmNext, qc ^ 1u, acc, pre);
     }
 }
 
@@ -175,7 +174,7 @@ __device__ void tdWarpItem(const PArgs& a, uint32_t item, uint32_t S, uint32_t q
 // edges per thread per round so their loads overlap.
 template <int NT>
 __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e1, uint32_t H, uint32_t qc,
-                           uint32_t level, GbPCounters* cur, uint32_t* bmNext, Acc& acc) {
+                           uint32_t level, GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre) {
     const unsigned long long* ho = a.ho[qc];
     if (threadIdx.x == 0) {
         uint32_t lo = ownerOf(ho, 0u, H - 1, (unsigned long long)e0);
@@ -198,7 +197,7 @@ __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e
             }
         }
 #pragma unroll
-        for (int k = 0; k < 2; ++k) discover(a, has[k], u[k], level, cur, bmNext, qc ^ 1u, acc);
+        for (int k = 0; k < 2; ++k) discover(a, has[k], u[k], level, cur, bmNext, qc ^ 1u, acc, pre);
     }
     __syncthreads();
 }
@@ -390,11 +389,22 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
     }
     const uint32_t endLevel = a.maxLevels ? a.startLevel + a.maxLevels : 0xFFFFFFFFu;
     uint64_t tPrev = globaltimer();
+    // The previous level's counters, read once after each barrier and carried
+    // into the next level in registers.
+    uint64_t nextSize, nextEdgesC, nextQ;
+    unsigned long long nextHub;
+    {
+        const GbPCounters* p0 = &a.ctr[(level + 2) % 3];
+        nextSize = ldv(&p0->found);
+        nextEdgesC = ldv(&p0->nextEdges);
+        nextQ = ldv(&p0->qtail);
+        nextHub = ldv(&p0->hubPack);
+    }
 
     for (;;) {
         GbPCounters* prev = &a.ctr[(level + 2) % 3];
         GbPCounters* cur = &a.ctr[level % 3];
-        const uint64_t size = ldv(&prev->found), fedges = ldv(&prev->nextEdges);
+        const uint64_t size = nextSize, fedges = nextEdgesC;
         if (size == 0 || level >= endLevel) break;
 
         // alpha/beta rule (src/cpu/bfs_cpu.cpp:247-279): always evaluated, it
@@ -444,18 +454,28 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
         if (strat == GB_STRAT_BU) {
             buLevel(a, level, acc);
         } else {
+            uint32_t S = (uint32_t)nextQ;
+            unsigned long long hp = nextHub;
             if (!qValid) {
                 bitmapToQueue<NT>(a, sm, level, prev);
                 if (!gridBarrier(bar, err, a.spinLimit)) return;
+                S = ldv(&prev->qtail);
+                hp = ldv(&prev->hubPack);
             }
             const uint32_t qc = level & 1u;
-            const uint32_t S = ldv(&prev->qtail);
-            const unsigned long long hp = ldv(&prev->hubPack);
             const uint32_t H = (uint32_t)(hp >> kHubShift);
             const uint64_t HE = hp & kHubMask;
-            const uint32_t per = strat == GB_STRAT_TD_WARP ? NT / 32 : NT;
-            const uint32_t nt = (S + per - 1) / per;
+            // warp per vertex: a static warp-strided loop over the queue (no
+            // tickets, no block barriers); edge-balanced tiles: block tickets
+            const bool warpMode = strat == GB_STRAT_TD_WARP;
+            if (warpMode) {
+                const uint64_t nwarps = gthreads >> 5;
+                for (uint64_t idx = gtid >> 5; idx < S; idx += nwarps)
+                    tdWarpEntry(a, (uint32_t)idx, qc, level, cur, a.bm[(level + 1) % 3], acc, fedges >= 65536);
+            }
+            const uint32_t nt = warpMode ? 0u : (S + NT - 1) / NT;
             const uint64_t HC = (uint64_t)NT * 2;
+            const bool pre = fedges >= 65536;
             const uint32_t nh = (uint32_t)((HE + HC - 1) / HC);
             uint32_t* bmNext = a.bm[(level + 1) % 3];
             // block b takes item b first; further items come from a ticket
@@ -467,14 +487,13 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
                 if (item >= nt + nh) break;
                 if (item < nt) {
                     switch (strat) {
-                        case GB_STRAT_TD_EPT1: tdTile<NT, 1>(a, sm, item, S, qc, level, cur, bmNext, acc); break;
-                        case GB_STRAT_TD_EPT4: tdTile<NT, 4>(a, sm, item, S, qc, level, cur, bmNext, acc); break;
-                        case GB_STRAT_TD_WARP: tdWarpItem<NT>(a, item, S, qc, level, cur, bmNext, acc); break;
-                        default: tdTile<NT, 2>(a, sm, item, S, qc, level, cur, bmNext, acc); break;
+                        case GB_STRAT_TD_EPT1: tdTile<NT, 1>(a, sm, item, S, qc, level, cur, bmNext, acc, pre); break;
+                        case GB_STRAT_TD_EPT4: tdTile<NT, 4>(a, sm, item, S, qc, level, cur, bmNext, acc, pre); break;
+                        default: tdTile<NT, 2>(a, sm, item, S, qc, level, cur, bmNext, acc, pre); break;
                     }
                 } else {
                     const uint64_t e0 = (uint64_t)(item - nt) * HC;
-                    tdHubChunk<NT>(a, sm, e0, min(e0 + HC, HE), H, qc, level, cur, bmNext, acc);
+                    tdHubChunk<NT>(a, sm, e0, min(e0 + HC, HE), H, qc, level, cur, bmNext, acc, pre);
                 }
             }
         }
@@ -498,6 +517,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
             tPrev = t;
         }
         const uint64_t found = ldv(&cur->found), nextE = ldv(&cur->nextEdges);
+        nextSize = found;
+        nextEdgesC = nextE;
+        nextQ = ldv(&cur->qtail);
+        nextHub = ldv(&cur->hubPack);
         reached += found;
         unexplored -= min(unexplored, nextE);
         if (bottomUp) {
@@ -581,6 +604,7 @@ using namespace gb;
 
 void gb_bfs::ensurePersistent(const gb_bfs_options& o) {
     const int block = o.block ? (int)o.block : 512;
+    pWant = (int)o.grid_blocks;
     const uint64_t hubCap = std::min<uint64_t>(n, m / 32 + 1);
     for (int i = 0; i < 2; ++i) {
         for (int j = 0; j < 3; ++j) pq[i][j].ensure(n);
@@ -601,9 +625,10 @@ void gb_bfs::ensurePersistent(const gb_bfs_options& o) {
         else
             GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, persistentBfsKernel<512>, 512, 0));
         if (perSm < 1) throw Error(GB_ERR_CUDA, "persistent BFS kernel cannot be resident");
-        pGrid = perSm * deviceSmCount();
+        pMax = perSm * deviceSmCount();
         pBlock = block;
     }
+    pGrid = pWant > 0 ? std::min(pWant, pMax) : pMax;
 }
 
 void gb_bfs::runPersistent(uint32_t src, const gb_bfs_options& o, std::vector<gb_level>* tr) {

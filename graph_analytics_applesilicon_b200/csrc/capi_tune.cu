@@ -144,12 +144,19 @@ int gb_bfs_autotune(gb_bfs* h, int variant, const uint32_t* sources, int k, gb_b
                     consider(c);
                 }
         } else if (variant == GB_BFS_PERSISTENT || variant == GB_BFS_BATCH) {
+            const int sms = deviceSmCount();
             for (uint32_t block : {256u, 512u})
                 for (uint32_t hub : {256u, 1024u, 4096u, 16384u}) {
                     c.block = block;
                     c.hub_min = hub;
+                    c.grid_blocks = 0;
                     consider(c);
                 }
+            c = best;  // then the grid size at the best block / hub cut
+            for (int frac : {4, 2}) {
+                c.grid_blocks = (uint32_t)std::max(1, sms / frac);
+                consider(c);
+            }
         } else {
             for (uint32_t tg : {128u, 256u, 512u, 1024u}) {
                 c.tg = tg;

@@ -379,6 +379,7 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
     o.beta = args.getDouble("beta", 18.0);
     o.block = (uint32_t)args.getInt("block", 512);
     o.hub_min = (uint32_t)args.getInt("hub-min", 4096);
+    o.grid_blocks = (uint32_t)args.getInt("grid-blocks", 0);
     const std::string sel = args.get("selector", "rule");
     if (sel != "rule" && sel != "learned") throw std::runtime_error("--selector must be rule or learned");
     o.selector = sel == "learned" ? GB_SELECT_LEARNED : GB_SELECT_RULE;

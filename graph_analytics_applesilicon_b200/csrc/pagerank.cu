@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 
 #include "pagerank.hpp"
 
@@ -41,8 +42,7 @@ struct PrArgs {
     double* contrib64[2];
     float* acc;
     float* accLo;
-    const uint32_t* list;  // adaptive: list0|list1|list2; GS natural: the list to sweep
-    uint32_t cnt[3];
+    const uint32_t* list;  // GS natural: the list to sweep
     GbPrControl* ctl;
     float* partF;
     double* partD;
@@ -50,6 +50,16 @@ struct PrArgs {
     float damping, base, invN;
     double base64, invN64, damping64;
     uint32_t lo, hi;  // GS colored: id range of the set
+    // split vertices: chunk table, per-hub (first, count), tickets, partials
+    const uint4* chunks;
+    const uint32_t* hubFirst;
+    unsigned* hubDone;
+    float* hubPart;   // indexed by global chunk index
+    uint32_t nChunks;
+    uint32_t chunkBase;  // global chunk index of chunks[0]
+    // degree classes of the relabeled layout: ids [binLo, binHi) use groups of binG lanes
+    uint32_t binLo[8], binHi[8], binG[8];
+    int nBins;
 };
 
 struct Kahan {
@@ -274,6 +284,62 @@ __device__ __forceinline__ float gatherSerial(const uint32_t* __restrict__ ci, c
     return k.sum;
 }
 
+// Kahan sum of contrib over [b, e) by group rank `rank` of G lanes (runtime
+// G), 16-byte aligned vector loads of col_idx.
+template <bool COHERENT>
+__device__ __forceinline__ float gatherGroup(const uint32_t* __restrict__ ci, const float* contrib, uint32_t b,
+                                             uint32_t e, unsigned rank, unsigned G) {
+    // Two 16-byte vectors per lane per step (8 gathers in flight); entries
+    // are added in the same per-lane order as a one-vector loop.
+    Kahan k;
+    const uint32_t step = 4 * G;
+    for (uint32_t i = (b & ~3u) + 4 * rank; i < e; i += 2 * step) {
+        const uint32_t j = i + step;
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(ci + i));
+        const uint4 r = j < e ? __ldg(reinterpret_cast<const uint4*>(ci + j)) : make_uint4(0, 0, 0, 0);
+        const float a0 = (i >= b) ? ldContrib<COHERENT>(contrib + q.x) : 0.f;
+        const float a1 = (i + 1 >= b && i + 1 < e) ? ldContrib<COHERENT>(contrib + q.y) : 0.f;
+        const float a2 = (i + 2 >= b && i + 2 < e) ? ldContrib<COHERENT>(contrib + q.z) : 0.f;
+        const float a3 = (i + 3 >= b && i + 3 < e) ? ldContrib<COHERENT>(contrib + q.w) : 0.f;
+        const float b0 = (j < e) ? ldContrib<COHERENT>(contrib + r.x) : 0.f;
+        const float b1 = (j + 1 < e) ? ldContrib<COHERENT>(contrib + r.y) : 0.f;
+        const float b2 = (j + 2 < e) ? ldContrib<COHERENT>(contrib + r.z) : 0.f;
+        const float b3 = (j + 3 < e) ? ldContrib<COHERENT>(contrib + r.w) : 0.f;
+        k.add(a0);
+        k.add(a1);
+        k.add(a2);
+        k.add(a3);
+        k.add(b0);
+        k.add(b1);
+        k.add(b2);
+        k.add(b3);
+    }
+    return k.sum;
+}
+
+// One warp chunk of a split vertex: the warp's sum goes to the chunk's
+// partial; the warp finishing the vertex's last chunk (ticket per vertex)
+// adds the partials in chunk order (Kahan) and stores the vertex.  All 32
+// lanes call it; store() runs on lane 0.
+template <bool COHERENT, class Store>
+__device__ __forceinline__ void chunkTask(const PrArgs& a, uint32_t t, const float* contrib, Store store) {
+    const uint4 c = a.chunks[t];  // vertex, start, end, hub
+    float s = gatherGroup<COHERENT>(a.ci, contrib, c.y, c.z, laneId(), 32);
+    s = warpSum(s);
+    if (laneId() == 0) {
+        a.hubPart[a.chunkBase + t] = s;
+        __threadfence();
+        const uint32_t first = a.hubFirst[2 * c.w], cnt = a.hubFirst[2 * c.w + 1];
+        if (atomicAdd(&a.hubDone[c.w], 1u) == cnt - 1) {
+            __threadfence();
+            Kahan k;
+            for (uint32_t i = 0; i < cnt; ++i) k.add(__ldcg(&a.hubPart[first + i]));
+            a.hubDone[c.w] = 0;
+            store(c.x, k.sum);
+        }
+    }
+}
+
 __device__ __forceinline__ float blockSum(float x, float* sm) {
     x = warpSum(x);
     const unsigned lane = laneId(), wid = threadIdx.x >> 5;
@@ -326,33 +392,30 @@ __global__ void prPullKernel(PrArgs a) {
             if (laneId() == 0) store((uint32_t)v, s);
         }
     } else {
-        const uint32_t* l0 = a.list;
-        const uint32_t* l1 = l0 + a.cnt[0];
-        const uint32_t* l2 = l1 + a.cnt[1];
-        for (uint32_t i = blockIdx.x; i < a.cnt[2]; i += gridDim.x) {  // large: block per vertex
-            const uint32_t v = l2[i];
-            const uint32_t b = a.rp[v], e = a.rp[v + 1];
-            Kahan k;
-            for (uint32_t j = (b & ~3u) + 4 * threadIdx.x; j < e; j += 4 * blockDim.x) {
-                const uint4 q = __ldg(reinterpret_cast<const uint4*>(a.ci + j));
-                if (j >= b) k.add(ldContrib<INPLACE>(contrib + q.x));
-                if (j + 1 >= b && j + 1 < e) k.add(ldContrib<INPLACE>(contrib + q.y));
-                if (j + 2 >= b && j + 2 < e) k.add(ldContrib<INPLACE>(contrib + q.z));
-                if (j + 3 >= b && j + 3 < e) k.add(ldContrib<INPLACE>(contrib + q.w));
-            }
-            const float s = blockSum(k.sum, sRed);
-            if (threadIdx.x == 0) store(v, s);
-        }
+        // degree-adaptive over the hub-first relabeled graph: task space =
+        // chunks of split vertices, then warp tasks of each degree class
+        uint64_t total = a.nChunks;
+        for (int b = 0; b < a.nBins; ++b) total += ((uint64_t)(a.binHi[b] - a.binLo[b]) * a.binG[b] + 31) / 32;
         const uint64_t nwarps = gthreads >> 5;
-        for (uint64_t i = gtid >> 5; i < a.cnt[1]; i += nwarps) {  // medium: warp per vertex
-            const uint32_t v = l1[i];
-            float s = gatherStrided<32, INPLACE>(a.ci, contrib, a.rp[v], a.rp[v + 1], laneId());
-            s = warpSum(s);
-            if (laneId() == 0) store(v, s);
-        }
-        for (uint64_t i = gtid; i < a.cnt[0]; i += gthreads) {  // small: thread per vertex
-            const uint32_t v = l0[i];
-            store(v, gatherSerial<INPLACE>(a.ci, contrib, a.rp[v], a.rp[v + 1]));
+        const unsigned lane = laneId();
+        for (uint64_t t = gtid >> 5; t < total; t += nwarps) {  // warp-uniform
+            if (t < a.nChunks) {
+                chunkTask<INPLACE>(a, (uint32_t)t, contrib, store);
+                continue;
+            }
+            uint64_t tb = t - a.nChunks;
+            int b = 0;
+            for (; b < a.nBins; ++b) {
+                const uint64_t nt = ((uint64_t)(a.binHi[b] - a.binLo[b]) * a.binG[b] + 31) / 32;
+                if (tb < nt) break;
+                tb -= nt;
+            }
+            const unsigned G = a.binG[b];
+            const uint32_t v = a.binLo[b] + (uint32_t)tb * (32 / G) + lane / G;
+            const bool active = v < a.binHi[b];
+            float s = active ? gatherGroup<INPLACE>(a.ci, contrib, a.rp[v], a.rp[v + 1], lane & (G - 1), G) : 0.f;
+            for (unsigned o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+            if (active && (lane & (G - 1)) == 0) store(v, s);
         }
     }
     if (!INPLACE) finishBlock<0>(a, acc);
@@ -360,6 +423,7 @@ __global__ void prPullKernel(PrArgs a) {
 
 // In-place sweep over a vertex list, warp per vertex (natural GS order; the
 // deferred mutual-pair partners form a second list swept afterwards).
+// Vertices with >= kGsHubMin in-edges are swept by gsHubKernel instead.
 __global__ void gsSweepListKernel(PrArgs a, uint32_t count) {
     const GbPrControl* c = a.ctl;
     if (ldvi(&c->stopped)) return;
@@ -368,10 +432,10 @@ __global__ void gsSweepListKernel(PrArgs a, uint32_t count) {
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < count; i += nwarps) {
         const uint32_t v = a.list[i];
-        Kahan k;
-        for (uint32_t j = a.rp[v] + laneId(); j < a.rp[v + 1]; j += 32)
-            k.add(*(volatile const float*)(a.contrib[0] + a.ci[j]));
-        const float s = warpSum(k.sum);
+        const uint32_t b = a.rp[v], e = a.rp[v + 1];
+        if (e - b >= kGsHubMin) continue;  // warp-uniform
+        float s = gatherGroup<true>(a.ci, a.contrib[0], b, e, laneId(), 32);
+        s = warpSum(s);
         if (laneId() == 0) {
             const float val = prValue(a, s, dang);
             a.r[cur ^ 1][v] = val;
@@ -381,22 +445,21 @@ __global__ void gsSweepListKernel(PrArgs a, uint32_t count) {
     }
 }
 
-// In-place sweep of one colour set [lo, hi) of the relabeled graph, thread
-// per vertex (colored GS order).
-__global__ void gsSweepSetKernel(PrArgs a) {
+// In-place sweep of the split vertices (natural GS order), warp per chunk.
+__global__ void gsHubKernel(PrArgs a) {
     const GbPrControl* c = a.ctl;
     if (ldvi(&c->stopped)) return;
     const int cur = c->cur;
     const float dang = c->dangHi + c->dangLo;
-    for (uint64_t v = a.lo + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.hi;
-         v += (uint64_t)gridDim.x * blockDim.x) {
-        Kahan k;
-        for (uint32_t j = a.rp[v]; j < a.rp[v + 1]; ++j) k.add(*(volatile const float*)(a.contrib[0] + a.ci[j]));
-        const float val = prValue(a, k.sum, dang);
+    auto store = [&](uint32_t v, float s) {
+        const float val = prValue(a, s, dang);
         a.r[cur ^ 1][v] = val;
         const uint32_t od = a.outdeg[v];
         a.contrib[0][v] = od ? val / (float)od : 0.0f;
-    }
+    };
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < a.nChunks; t += nwarps)
+        chunkTask<true>(a, (uint32_t)t, a.contrib[0], store);
 }
 
 // In-place variants: contributions and dangling mass of the current iterate.
@@ -570,8 +633,6 @@ PrArgs makeArgs(gb_pr& h, bool relabeled) {
     }
     a.acc = h.acc.get();
     a.accLo = h.accLo.get();
-    a.list = h.bins.get();
-    for (int i = 0; i < 3; ++i) a.cnt[i] = h.binCount[i];
     a.ctl = h.ctl.get();
     a.partF = h.partF.get();
     a.partD = h.partD.get();
@@ -585,6 +646,26 @@ uint32_t gridFor(uint64_t work, uint32_t threads) {
     return (uint32_t)std::max<uint64_t>(1, std::min(b, cap));
 }
 
+// Grid of exactly the blocks that can be resident at once (grid-stride
+// kernels: a second, partly filled wave would only add a tail).
+template <class K>
+uint32_t residentGrid(K kernel, uint64_t work, uint32_t threads) {
+    static std::map<std::pair<const void*, uint32_t>, int> cache;
+    auto key = std::make_pair((const void*)kernel, threads);
+    auto it = cache.find(key);
+    int perSm;
+    if (it == cache.end()) {
+        GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, (int)threads, 0));
+        perSm = std::max(perSm, 1);
+        cache[key] = perSm;
+    } else {
+        perSm = it->second;
+    }
+    uint64_t b = (work + threads - 1) / threads;
+    uint64_t cap = std::min<uint64_t>(kMaxGrid, (uint64_t)deviceSmCount() * perSm);
+    return (uint32_t)std::max<uint64_t>(1, std::min(b, cap));
+}
+
 }  // namespace
 
 // Enqueue one iteration of `variant` on the handle's stream (capturable).
@@ -593,10 +674,11 @@ static void enqueueIteration(gb_pr& h, int v, const gb_pr_options& o, PrArgs& a,
     cudaStream_t s = h.stream.s;
     const uint32_t gN = gridFor(h.n, 256);
     auto pullGrid = [&](int mode) {
-        if (mode == 0) return gridFor(h.n, tg);
-        if (mode == 1) return gridFor(h.n * 32, tg);
-        return gridFor(std::max<uint64_t>({(uint64_t)h.binCount[0], (uint64_t)h.binCount[1] * 32,
-                                           (uint64_t)h.binCount[2] * tg}), tg);
+        if (mode == 0) return residentGrid(prPullKernel<0, false>, h.n, tg);
+        if (mode == 1) return residentGrid(prPullKernel<1, false>, h.n * 32, tg);
+        uint64_t tasks = h.nChunks;  // adaptive: warp tasks
+        for (int b = 0; b < h.nBins; ++b) tasks += ((uint64_t)(h.binHi[b] - h.binLo[b]) * h.binG[b] + 31) / 32;
+        return residentGrid(prPullKernel<2, false>, tasks * 32, tg);
     };
     const bool inplace = v == GB_PR_PULL_GS || (o.inplace && v != GB_PR_PUSH && v != GB_PR_PULL_F64);
     if (v == GB_PR_PUSH) {
@@ -607,27 +689,49 @@ static void enqueueIteration(gb_pr& h, int v, const gb_pr_options& o, PrArgs& a,
     } else if (!inplace) {
         if (v == GB_PR_PULL_SCALAR) prPullKernel<0, false><<<pullGrid(0), tg, 0, s>>>(a);
         else if (v == GB_PR_PULL_VECTOR) prPullKernel<1, false><<<pullGrid(1), tg, 0, s>>>(a);
-        else prPullKernel<2, false><<<pullGrid(2), tg, 0, s>>>(a);
+        else prPullKernel<2, false><<<pullGrid(2), tg, 0, s>>>(ag);
     } else {
         const bool colored = v == GB_PR_PULL_GS && h.gsColored;
-        PrArgs& w = colored ? ag : a;
+        PrArgs& w = (colored || v == GB_PR_PULL_ADAPTIVE) ? ag : a;
         gsContribKernel<<<gN, 256, 0, s>>>(w);
         if (v == GB_PR_PULL_GS) {
             if (colored) {
-                for (size_t k = 0; k + 1 < h.gsSetStart.size(); ++k) {
+                // one in-place sweep per colour set, in set order: the set's
+                // split hubs and degree classes in one task-space launch
+                for (const auto& L : h.gsSetLayout) {
                     PrArgs ws = w;
-                    ws.lo = h.gsSetStart[k];
-                    ws.hi = h.gsSetStart[k + 1];
-                    gsSweepSetKernel<<<gridFor(ws.hi - ws.lo, tg), tg, 0, s>>>(ws);
+                    ws.chunks = h.gsHubChunks.get() + L.chunk0;
+                    ws.nChunks = L.chunk1 - L.chunk0;
+                    ws.hubFirst = h.gsHubFirst.get();
+                    ws.hubDone = h.gsHubDone.get();
+                    ws.hubPart = h.gsHubPart.get();
+                    ws.chunkBase = L.chunk0;
+                    ws.nBins = L.nBins;
+                    uint64_t tasks = ws.nChunks;
+                    for (int b = 0; b < 8; ++b) {
+                        ws.binLo[b] = L.lo[b];
+                        ws.binHi[b] = L.hi[b];
+                        ws.binG[b] = L.g[b];
+                        if (b < L.nBins) tasks += ((uint64_t)(L.hi[b] - L.lo[b]) * L.g[b] + 31) / 32;
+                    }
+                    prPullKernel<2, true><<<residentGrid(prPullKernel<2, true>, tasks * 32, tg), tg, 0, s>>>(ws);
                 }
-            } else if (h.gsNatB > 0) {
+            } else {
                 PrArgs wa = w;
+                if (h.gsChunks) {
+                    wa.chunks = h.gsHubChunks.get();
+                    wa.hubFirst = h.gsHubFirst.get();
+                    wa.hubDone = h.gsHubDone.get();
+                    wa.hubPart = h.gsHubPart.get();
+                    wa.nChunks = h.gsChunks;
+                    gsHubKernel<<<gridFor((uint64_t)h.gsChunks * 32, tg), tg, 0, s>>>(wa);
+                }
                 wa.list = h.gsNat.get();
                 gsSweepListKernel<<<gridFor((uint64_t)h.gsNatA * 32, tg), tg, 0, s>>>(wa, h.gsNatA);
-                wa.list = h.gsNat.get() + h.gsNatA;
-                gsSweepListKernel<<<gridFor((uint64_t)h.gsNatB * 32, tg), tg, 0, s>>>(wa, h.gsNatB);
-            } else {
-                prPullKernel<1, true><<<pullGrid(1), tg, 0, s>>>(w);
+                if (h.gsNatB > 0) {
+                    wa.list = h.gsNat.get() + h.gsNatA;
+                    gsSweepListKernel<<<gridFor((uint64_t)h.gsNatB * 32, tg), tg, 0, s>>>(wa, h.gsNatB);
+                }
             }
         } else if (v == GB_PR_PULL_SCALAR) {
             prPullKernel<0, true><<<pullGrid(0), tg, 0, s>>>(w);
@@ -692,12 +796,27 @@ gb_pr_result gb_pr::run(int v, const gb_pr_options& o) {
     a.base64 = (1.0 - a.damping64) / (double)n;
     a.invN64 = 1.0 / (double)n;
     PrArgs ag = a;
-    if (gsColored && gsReady) {
+    if (v == GB_PR_PULL_ADAPTIVE) {  // hub-first relabeled layout
+        ag.rp = rowA.get();
+        ag.ci = colA.get();
+        ag.outdeg = outdegA.get();
+        ag.chunks = hubChunks.get();
+        ag.hubFirst = hubFirst.get();
+        ag.hubDone = hubDone.get();
+        ag.hubPart = hubPart.get();
+        ag.nChunks = nChunks;
+        ag.nBins = nBins;
+        for (int b = 0; b < 8; ++b) {
+            ag.binLo[b] = binLo[b];
+            ag.binHi[b] = binHi[b];
+            ag.binG[b] = binG[b];
+        }
+    } else if (gsColored && gsReady) {
         ag.rp = rowGS.get();
         ag.ci = colGS.get();
         ag.outdeg = outdegGS.get();
     }
-    const bool relabel = v == GB_PR_PULL_GS && gsColored;
+    const bool relabel = (v == GB_PR_PULL_GS && gsColored) || v == GB_PR_PULL_ADAPTIVE;
     GB_CUDA(cudaEventRecord(ev.a, stream.s));
     GB_CUDA(cudaMemcpyAsync(ctl.get(), &c, sizeof c, cudaMemcpyHostToDevice, stream.s));
     if (v == GB_PR_PUSH) {
@@ -759,13 +878,16 @@ void gb_pr::ranks(float* out) {
     if (lastVariant == GB_PR_PULL_F64) throw Error(GB_ERR_STATE, "last run was FP64: use the double ranks");
     GbPrControl hc{};
     GB_CUDA(cudaMemcpy(&hc, ctl.get(), sizeof hc, cudaMemcpyDeviceToHost));
-    if (!gsLastRun) {
+    const std::vector<uint32_t>* map = lastVariant == GB_PR_PULL_ADAPTIVE ? &permA : gsLastRun ? &gsNewId : nullptr;
+    if (!map) {
         GB_CUDA(cudaMemcpy(out, r[hc.cur].get(), n * 4, cudaMemcpyDeviceToHost));
         return;
     }
-    std::vector<float> tmp(n);
+    std::vector<float> tmp(n);  // relabeled layout: back to the caller's ids
     GB_CUDA(cudaMemcpy(tmp.data(), r[hc.cur].get(), n * 4, cudaMemcpyDeviceToHost));
-    for (uint64_t v = 0; v < n; ++v) out[v] = tmp[gsNewId[v]];
+    const uint32_t* m = map->data();
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < (int64_t)n; ++v) out[v] = tmp[m[v]];
 }
 
 void gb_pr::ranks64(double* out) {

@@ -8,6 +8,8 @@
 
 #include "common.cuh"
 
+constexpr uint32_t kGsHubMin = 4096;  // natural-order GS: split vertices with this many in-edges
+
 // Iteration control, updated on the device by the last block of every
 // iteration kernel: which rank buffer is current, how many iterations ran,
 // and the tol-mode stop rule (L1 change, max relative change, stagnation
@@ -45,11 +47,33 @@ struct gb_pr {
     gb::EventPair ev;
     std::vector<uint32_t> hostRowIn, hostColIn, hostOutdeg;
 
-    // adaptive bins (in-degree): one buffer holding list0 | list1 | list2
-    gb::DevBuf<uint32_t> bins;
-    uint32_t binCount[3] = {0, 0, 0};
+    // adaptive pull: hub-first relabeled in-CSR (new id = rank by descending
+    // in-degree), so every degree bin is a contiguous id range
+    gb::DevBuf<uint32_t> rowA, colA, outdegA;
+    gb::DevBuf<uint4> hubChunks;     // (vertex, start, end, hub index) per chunk
+    gb::DevBuf<uint32_t> hubFirst;   // per hub: first chunk | chunk count
+    gb::DevBuf<unsigned> hubDone;    // per hub: chunks finished (reset by the last)
+    gb::DevBuf<float> hubPart;       // per chunk: Kahan sum, compensation
+    std::vector<uint32_t> permA;     // old id -> new id
+    uint32_t nHubs = 0, nChunks = 0;
+    uint32_t binLo[8] = {0}, binHi[8] = {0}, binG[8] = {0};  // group-size ranges (G = 1..32)
+    int nBins = 0;
     uint32_t binSmall = 0, binLarge = 0;
     bool binsReady = false;
+    // Gauss-Seidel natural order: vertices of in-degree >= kGsHubMin are split
+    // into warp chunks (natural ids) and swept first, in place
+    gb::DevBuf<uint4> gsHubChunks;
+    gb::DevBuf<uint32_t> gsHubFirst;
+    gb::DevBuf<unsigned> gsHubDone;
+    gb::DevBuf<float> gsHubPart;
+    uint32_t gsHubs = 0, gsChunks = 0;
+    // colored order: per colour set, its degree classes and its chunk range
+    struct GsSetLayout {
+        uint32_t lo[8], hi[8], g[8];
+        int nBins;
+        uint32_t chunk0, chunk1;
+    };
+    std::vector<GsSetLayout> gsSetLayout;
 
     // Gauss-Seidel order (prepareGS)
     bool gsReady = false, gsColored = false;

@@ -130,6 +130,8 @@ typedef struct {
     uint32_t hub_min;    /* persistent: degree at which a vertex is split across blocks */
     uint32_t block;      /* persistent / batched: threads per block (256 or 512) */
     uint64_t spin_limit; /* grid-barrier wait bound in polls (0 = default, ~ seconds) */
+    uint32_t grid_blocks; /* persistent / batched: blocks in the grid (0 = every resident block) */
+    uint32_t pad_;
 } gb_bfs_options;
 
 void gb_bfs_default_options(gb_bfs_options* o);
@@ -197,7 +199,7 @@ int gb_bfs_profile_batch_levels(gb_bfs* h, const uint32_t* sources, int k, const
 
 /* Autotuner (replaces scripts/sweep_balanced.sh, sweep_tg.sh, sweep_do.sh):
  * times candidate small_max/large_min and tg (gpu_binned), ept and tg
- * (gpu_edge, gpu_do), block size and hub_min cut (persistent, GB_BFS_BATCH)
+ * (gpu_edge, gpu_do), block size, grid size and hub_min cut (persistent, GB_BFS_BATCH)
  * on the given sources and writes the fastest into *o. */
 int gb_bfs_autotune(gb_bfs* h, int variant, const uint32_t* sources, int k, gb_bfs_options* o);
 
