@@ -726,8 +726,22 @@ static void enqueueIteration(gb_pr& h, int v, const gb_pr_options& o, PrArgs& a,
                     wa.nChunks = h.gsChunks;
                     gsHubKernel<<<gridFor((uint64_t)h.gsChunks * 32, tg), tg, 0, s>>>(wa);
                 }
-                wa.list = h.gsNat.get();
-                gsSweepListKernel<<<gridFor((uint64_t)h.gsNatA * 32, tg), tg, 0, s>>>(wa, h.gsNatA);
+                // The main list runs as kGsNatSlices consecutive launches in
+                // list order, so every slice reads the finished values of
+                // all earlier ones.  One launch of the whole list puts every
+                // vertex of a small graph into a single wave whose reads of
+                // one another are a random mix of old and new values; its
+                // per-sweep change then understates the remaining error
+                // (rmat12, K = 0: top-1000 relative error up to 1.1e-3 when
+                // stopped at L1 change 2.5e-7, 30-36 sweeps; in slices the
+                // same stop gives about 3e-4 in about 21 sweeps).
+                const uint32_t slices = h.gsNatA >= kGsNatSlices * 32u ? kGsNatSlices : 1u;
+                for (uint32_t k = 0; k < slices; ++k) {
+                    const uint32_t lo = (uint32_t)((uint64_t)h.gsNatA * k / slices);
+                    const uint32_t hi = (uint32_t)((uint64_t)h.gsNatA * (k + 1) / slices);
+                    wa.list = h.gsNat.get() + lo;
+                    gsSweepListKernel<<<gridFor((uint64_t)(hi - lo) * 32, tg), tg, 0, s>>>(wa, hi - lo);
+                }
                 if (h.gsNatB > 0) {
                     wa.list = h.gsNat.get() + h.gsNatA;
                     gsSweepListKernel<<<gridFor((uint64_t)h.gsNatB * 32, tg), tg, 0, s>>>(wa, h.gsNatB);

@@ -9,6 +9,7 @@
 #include "common.cuh"
 
 constexpr uint32_t kGsHubMin = 4096;  // natural-order GS: split vertices with this many in-edges
+constexpr uint32_t kGsNatSlices = 8;    // natural-order GS: the main list runs as this many ordered launches
 
 // Iteration control, updated on the device by the last block of every
 // iteration kernel: which rank buffer is current, how many iterations ran,
