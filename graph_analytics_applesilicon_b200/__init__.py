@@ -163,6 +163,7 @@ def lib():
             "gb_pr_autotune": (C.c_int, [vp, C.POINTER(PrOptions)]),
             "gb_pr_stream": (vp, [vp]),
             "gb_prim_scan": (C.c_int, [_u32p, C.c_uint64, _u32p, C.POINTER(C.c_uint32)]),
+            "gb_prim_scan_device_noalloc": (C.c_int, [vp, C.c_uint64, vp, vp, vp, vp]),
             "gb_prim_reduce": (C.c_int, [_u32p, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
             "gb_prim_queue_bitmap": (C.c_int, [_u32p, C.c_uint64, C.c_uint64, _u32p, _u32p,
                                                C.POINTER(C.c_uint64)]),
@@ -538,6 +539,15 @@ def prim_scan(x: np.ndarray):
     tot = C.c_uint32(0)
     check(lib().gb_prim_scan(x if x.size else np.zeros(1, np.uint32), x.size, out, C.byref(tot)))
     return out[: x.size], tot.value
+
+
+def prim_scan_device_noalloc(in_ptr: int, n: int, out_ptr: int, total_ptr: int = 0, flag_ptr: int = 0,
+                             stream: int = 0):
+    """Exclusive scan of n uint32 at device address in_ptr into out_ptr, with
+    no device allocation (gb_prim_scan_device_noalloc); only enqueues on
+    stream.  Pointers are plain device addresses (0 = none)."""
+    check(lib().gb_prim_scan_device_noalloc(in_ptr or None, n, out_ptr or None, total_ptr or None,
+                                            flag_ptr or None, stream or None))
 
 
 def prim_reduce(x: np.ndarray):

@@ -10,6 +10,11 @@
 // warp-aggregated appends.
 #include "prims.cuh"
 
+#include <mutex>
+#include <string>
+
+#include "capi_util.hpp"
+
 namespace gb {
 
 namespace {
@@ -246,3 +251,92 @@ void fillU32(uint32_t* p, uint32_t value, uint64_t n, cudaStream_t st) {
 }
 
 }  // namespace gb
+
+// ------------------------------------------------------------------------
+// Exclusive scan into caller-owned device memory that allocates nothing.
+//
+// scanExclusive above takes its look-back scratch from a buffer the caller's
+// handle grows on demand.  Some callers cannot allocate device memory at the
+// point where they need a scan: a host program that hands the whole GPU memory
+// to its own pool at start-up and has none left to give, or a stream pipeline
+// that must not call cudaMalloc / cudaFree between launches because those
+// calls can wait for the whole device.  For them the same single-pass kernel
+// runs here with its scratch in a fixed array in this module's global memory,
+// which the CUDA runtime places when the module loads.
+//
+// Limits and rules (repeated in include/graph_b200.h):
+//  * n <= kNoAllocScanMax (4096 tiles of 2048 elements = 8,388,608); larger n
+//    is rejected with GB_ERR_CAPACITY before anything is enqueued.
+//  * Every status word of the tiles in use, the tile ticket and the timeout
+//    word must be zero when the kernel starts; each call clears them on its
+//    stream (cudaMemsetAsync, which allocates nothing) before the launch.
+//  * There is one scratch array per device, so two calls whose kernels
+//    overlap on the same GPU (different streams, or host threads) race on it
+//    and both results are undefined.  Order them on one stream or with events.
+//  * The first call on a device looks up the array's device address
+//    (cudaGetSymbolAddress, once per device, with that device current); make
+//    that first call before any stream capture begins.
+// ------------------------------------------------------------------------
+// [0, 4096): per-tile look-back status words; [4096]: tile ticket (low 32
+// bits) and timeout flag (high 32 bits).  32 KiB + 8 bytes per device.
+static __device__ __align__(256) unsigned long long gNoAllocScanScratch[4096 + 1];
+
+namespace gb {
+namespace {
+
+constexpr uint32_t kNoAllocScanTiles = 4096;  // the size of gNoAllocScanScratch - 1
+constexpr uint64_t kNoAllocScanMax = (uint64_t)kNoAllocScanTiles * kScanTile;
+static_assert(sizeof(gNoAllocScanScratch) == (kNoAllocScanTiles + 1) * sizeof(unsigned long long),
+              "scratch array and tile limit disagree");
+constexpr int kNoAllocMaxDevices = 64;
+
+std::mutex gNoAllocMu;
+unsigned long long* gNoAllocScratchPtr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device; looked up on
+// the first call for that device and remembered.
+unsigned long long* noAllocScanScratch() {
+    int dev = 0;
+    GB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        throw Error(GB_ERR_ARG, "no-allocation scan supports device ordinals below 64");
+    std::lock_guard<std::mutex> lock(gNoAllocMu);
+    if (!gNoAllocScratchPtr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, gNoAllocScanScratch);
+        if (e != cudaSuccess || !p)
+            throw Error(GB_ERR_CUDA, std::string("cudaGetSymbolAddress(scan scratch) failed: ") +
+                                         cudaGetErrorString(e));
+        gNoAllocScratchPtr[dev] = static_cast<unsigned long long*>(p);
+    }
+    return gNoAllocScratchPtr[dev];
+}
+
+}  // namespace
+}  // namespace gb
+
+extern "C" int gb_prim_scan_device_noalloc(const uint32_t* in, uint64_t n, uint32_t* out, uint32_t* total,
+                                           uint32_t* timeout_flag, void* stream) {
+    using namespace gb;
+    return guard([&] {
+        GB_REQUIRE(n == 0 || (in && out), "null argument");
+        if (n > kNoAllocScanMax)
+            throw Error(GB_ERR_CAPACITY, "no-allocation scan: n = " + std::to_string(n) + " exceeds its limit of " +
+                                             std::to_string(kNoAllocScanMax) + " elements");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        unsigned long long* scratch = noAllocScanScratch();
+        unsigned* counters = reinterpret_cast<unsigned*>(scratch + kNoAllocScanTiles);
+        if (n == 0) {
+            if (total) GB_CUDA(cudaMemsetAsync(total, 0, 4, st));
+            if (timeout_flag) GB_CUDA(cudaMemsetAsync(timeout_flag, 0, 4, st));
+            return;
+        }
+        const uint32_t tiles = divUp(n, kScanTile);
+        GB_CUDA(cudaMemsetAsync(scratch, 0, (size_t)tiles * sizeof(unsigned long long), st));
+        GB_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned), st));
+        scanKernel<<<tiles, kScanThreads, 0, st>>>(in, out, n, total, scratch, counters);
+        GB_LAUNCH_CHECK();
+        if (timeout_flag)
+            GB_CUDA(cudaMemcpyAsync(timeout_flag, counters + 1, sizeof(unsigned), cudaMemcpyDeviceToDevice, st));
+    });
+}

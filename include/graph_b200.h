@@ -263,6 +263,27 @@ void* gb_pr_stream(const gb_pr* h);
 /* Exclusive scan / sum / max of uint32 (src/metal/primitives.hpp:18-65),
  * host arrays in and out; total may be NULL. */
 int gb_prim_scan(const uint32_t* in, uint64_t n, uint32_t* out, uint32_t* total);
+/* Exclusive scan of device memory that allocates no device memory.  It has no
+ * counterpart in the reference (src/metal/primitives.mm:69-101 allocates its
+ * block-sum buffers per call); it exists for callers that cannot allocate at
+ * the point of the scan, such as a program whose device memory is all held by
+ * its own pool, or a stream pipeline that must avoid cudaMalloc / cudaFree
+ * because they can wait for the whole device.
+ *   in, out (in == out allowed), total, timeout_flag: device pointers on the
+ *   current device; total and timeout_flag may be NULL.  out[i] = in[0] + ...
+ *   + in[i-1] (mod 2^32), *total = sum of all n; *timeout_flag = 1 if a
+ *   look-back wait ran out (the result is then invalid), else 0.
+ *   stream: a cudaStream_t (NULL = the default stream).  The call only
+ *   enqueues work: results are ready when the stream reaches them.
+ * Limit: n <= 8,388,608 (4096 tiles of 2048); larger n returns
+ * GB_ERR_CAPACITY and enqueues nothing.  The look-back scratch is one fixed
+ * 32 KiB array per device inside the library, cleared on the stream by each
+ * call before its kernel; calls whose kernels overlap on the same GPU (other
+ * streams, other host threads) race on it and give undefined results, so
+ * order them.  The first call on each device looks up that array's address
+ * with the device current; make it before any stream capture begins. */
+int gb_prim_scan_device_noalloc(const uint32_t* in, uint64_t n, uint32_t* out, uint32_t* total,
+                                uint32_t* timeout_flag, void* stream);
 int gb_prim_reduce(const uint32_t* in, uint64_t n, uint32_t* sum, uint32_t* max);
 /* queueToBitmap then bitmapToQueue (src/metal/primitives.mm:103-123). */
 int gb_prim_queue_bitmap(const uint32_t* queue, uint64_t size, uint64_t n, uint32_t* bitmap_out,
