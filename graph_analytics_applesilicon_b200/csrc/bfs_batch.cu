@@ -91,11 +91,36 @@ struct BSmem {
     unsigned long long f[NT];
     float sel[kSelParams];
     unsigned long long acc[6];
+    unsigned long long cnt[7];  // counters after a barrier (see batchBarrier)
     uint32_t range[2];
     unsigned item;
     int strat;
     uint32_t base;
+    int ok;
 };
+
+// Grid barrier after which every thread of the block sees counters *c in
+// sm.cnt (found, aedges, fullEdges, fullCount, acnt, hubPack, ccnt), read
+// once per block by thread 0 instead of once per warp.
+template <int NT>
+__device__ __forceinline__ bool batchBarrier(const BArgs& a, BSmem<NT>& sm, const BCounters* c) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const bool ok = gridArriveWait(&a.ctl[0], &a.ctl[1], a.spinLimit, gridDim.x);
+        sm.ok = ok;
+        if (ok) {
+            sm.cnt[0] = ldv64(&c->found);
+            sm.cnt[1] = ldv64(&c->aedges);
+            sm.cnt[2] = ldv64(&c->fullEdges);
+            sm.cnt[3] = ldv64(&c->fullCount);
+            sm.cnt[4] = ldv32(&c->acnt);
+            sm.cnt[5] = ldv64(&c->hubPack);
+            sm.cnt[6] = ldv32(&c->ccnt);
+        }
+    }
+    __syncthreads();
+    return sm.ok != 0;
+}
 
 // Write depth `level` for the sources in b (lanes of a warp call together;
 // consecutive vertices give coalesced stores per source).
@@ -259,7 +284,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
     unsigned* err = &a.ctl[1];
     const bool learned = a.selector == GB_SELECT_LEARNED && a.sel != nullptr;
     if (learned)
-        for (int i = tid; i < kSelParams; i += NT) sm.sel[i] = a.sel[i];
+        selectorStage(sm.sel, a.sel, tid, NT);
 
     // prologue: masks zeroed, counters zeroed, then the sources
     for (uint64_t v = gtid; v < a.n; v += gthreads) {
@@ -297,18 +322,21 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
             }
         }
     }
-    if (!gridBarrier(bar, err, a.spinLimit)) return;
+    if (!batchBarrier<NT>(a, sm, &a.ctr[3])) return;
 
     uint32_t level = 0;
     bool bottomUp = false;
-    uint64_t scout = ldv64(&a.ctr[3].aedges), toCheck = a.m, fullEdges = 0, fullCount = 0;
+    uint64_t scout = sm.cnt[1], toCheck = a.m, fullEdges = 0, fullCount = 0;
     int lastStrat = -1;
     uint64_t tPrev = globaltimer();
+    // The last two levels' outputs, carried in registers: (size, fedges,
+    // qCount, qHub) of level-1 and (q2Count, q2Hub) of level-2.
+    uint64_t size = sm.cnt[0], fedges = sm.cnt[1];
+    uint32_t qCount = (uint32_t)sm.cnt[4], q2Count = 0;
+    unsigned long long qHub = sm.cnt[5], q2Hub = 0;
     for (;;) {
         BCounters* prev = &a.ctr[(level + 3) & 3];
-        BCounters* prev2 = &a.ctr[(level + 2) & 3];
         BCounters* cur = &a.ctr[level & 3];
-        const uint64_t size = ldv64(&prev->found), fedges = ldv64(&prev->aedges);
         if (size == 0) break;
         if (!bottomUp && (double)scout > (double)toCheck / a.alpha) bottomUp = true;
         if (!bottomUp) toCheck -= min(toCheck, scout);
@@ -386,13 +414,13 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
             // phase A: clear the previous level's frontier entries of fr[nq]
             // (its active list is still intact), then push.
             {
-                const uint32_t P = ldv32(&prev2->acnt);
+                const uint32_t P = q2Count;
                 for (uint64_t i = gtid; i < P; i += gthreads) a.fr[nq][a.qv[nq][i]] = 0;
-                const uint32_t PH = (uint32_t)(ldv64(&prev2->hubPack) >> kHubShift);
+                const uint32_t PH = (uint32_t)(q2Hub >> kHubShift);
                 for (uint64_t i = gtid; i < PH; i += gthreads) a.fr[nq][a.hv[nq][i]] = 0;
             }
-            const uint32_t S = ldv32(&prev->acnt);
-            const unsigned long long hp = ldv64(&prev->hubPack);
+            const uint32_t S = qCount;
+            const unsigned long long hp = qHub;
             const uint32_t H = (uint32_t)(hp >> kHubShift);
             const uint64_t HE = hp & kHubMask;
             const uint32_t per = strat == GB_STRAT_TD_WARP ? NT / 32 : NT;
@@ -417,9 +445,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                     pushHubChunk<NT>(a, sm, e0, min(e0 + HC, HE), H, qc, cur);
                 }
             }
-            if (!gridBarrier(bar, err, a.spinLimit)) return;
+            if (!batchBarrier<NT>(a, sm, cur)) return;
             // phase B: fold the candidates' pushed bits
-            const uint32_t C = ldv32(&cur->ccnt);
+            const uint32_t C = (uint32_t)sm.cnt[6];
             for (uint64_t base = (uint64_t)blockIdx.x * NT; base < C; base += gthreads) {
                 const uint64_t i = base + tid;
                 unsigned long long b = 0;
@@ -461,15 +489,19 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
             if (sm.acc[4]) atomicAdd(&cur->fullCount, sm.acc[4]);
             if (sm.acc[5]) atomicAdd(&cur->examined, sm.acc[5]);
         }
-        if (!gridBarrier(bar, err, a.spinLimit)) return;
+        if (!batchBarrier<NT>(a, sm, cur)) return;
         if (gtid == 0) {
             const uint64_t t = globaltimer();
             if (a.trace && level < a.traceCap) a.trace[level].time_ms = (double)(t - tPrev) * 1e-6;
             tPrev = t;
         }
-        const uint64_t found = ldv64(&cur->found), nextE = ldv64(&cur->aedges);
-        fullEdges += ldv64(&cur->fullEdges);
-        fullCount += ldv64(&cur->fullCount);
+        const uint64_t found = sm.cnt[0], nextE = sm.cnt[1];
+        fullEdges += sm.cnt[2];
+        fullCount += sm.cnt[3];
+        q2Count = qCount;
+        q2Hub = qHub;
+        qCount = (uint32_t)sm.cnt[4];
+        qHub = sm.cnt[5];
         if (bottomUp) {
             if (!(found >= size || (double)found > (double)a.n / a.beta)) {
                 bottomUp = false;
@@ -478,6 +510,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
         } else {
             scout = nextE;
         }
+        size = found;
+        fedges = nextE;
         lastStrat = strat;
         ++level;
     }

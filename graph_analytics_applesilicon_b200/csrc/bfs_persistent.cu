@@ -115,11 +115,33 @@ struct Smem {
     uint32_t st[NT];
     float sel[kSelParams];
     unsigned long long acc[3];
+    unsigned long long cnt[4];  // level counters after a barrier: found, nextEdges, qtail, hubPack
     uint32_t range[2];
     unsigned item;
     int strat;
     uint32_t base;
+    int ok;
 };
+
+// Grid barrier after which every thread of the block sees counters *c in
+// sm.cnt: thread 0 reads them once for its block, so a level costs one L2
+// request per block on the counters' line rather than one per warp.
+template <int NT>
+__device__ __forceinline__ bool barrierWithCounters(const PArgs& a, Smem<NT>& sm, const GbPCounters* c) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const bool ok = gridArriveWait(&a.ctl[0], &a.ctl[1], a.spinLimit, gridDim.x);
+        sm.ok = ok;
+        if (ok) {
+            sm.cnt[0] = ldv(&c->found);
+            sm.cnt[1] = ldv(&c->nextEdges);
+            sm.cnt[2] = ldv(&c->qtail);
+            sm.cnt[3] = ldv(&c->hubPack);
+        }
+    }
+    __syncthreads();
+    return sm.ok != 0;
+}
 
 // Edge-balanced expansion of one tile of NT queue entries: the entries'
 // degrees are scanned in shared memory and every thread takes EPT edges per
@@ -325,7 +347,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
     unsigned* err = &a.ctl[1];
     const bool learned = a.selector == GB_SELECT_LEARNED && a.sel != nullptr;
     if (learned)
-        for (int i = tid; i < kSelParams; i += NT) sm.sel[i] = a.sel[i];
+        selectorStage(sm.sel, a.sel, tid, NT);
 
     uint32_t level;
     bool bottomUp, qValid;
@@ -458,9 +480,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
             unsigned long long hp = nextHub;
             if (!qValid) {
                 bitmapToQueue<NT>(a, sm, level, prev);
-                if (!gridBarrier(bar, err, a.spinLimit)) return;
-                S = ldv(&prev->qtail);
-                hp = ldv(&prev->hubPack);
+                if (!barrierWithCounters<NT>(a, sm, prev)) return;
+                S = (uint32_t)sm.cnt[2];
+                hp = sm.cnt[3];
             }
             const uint32_t qc = level & 1u;
             const uint32_t H = (uint32_t)(hp >> kHubShift);
@@ -510,17 +532,17 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
             if (sm.acc[1]) atomicAdd(&cur->nextEdges, sm.acc[1]);
             if (sm.acc[2]) atomicAdd(&cur->examined, sm.acc[2]);
         }
-        if (!gridBarrier(bar, err, a.spinLimit)) return;
+        if (!barrierWithCounters<NT>(a, sm, cur)) return;
         if (gtid == 0) {
             const uint64_t t = globaltimer();
             if (a.trace && level < a.traceCap) a.trace[level].time_ms = (double)(t - tPrev) * 1e-6;
             tPrev = t;
         }
-        const uint64_t found = ldv(&cur->found), nextE = ldv(&cur->nextEdges);
+        const uint64_t found = sm.cnt[0], nextE = sm.cnt[1];
         nextSize = found;
         nextEdgesC = nextE;
-        nextQ = ldv(&cur->qtail);
-        nextHub = ldv(&cur->hubPack);
+        nextQ = sm.cnt[2];
+        nextHub = sm.cnt[3];
         reached += found;
         unexplored -= min(unexplored, nextE);
         if (bottomUp) {

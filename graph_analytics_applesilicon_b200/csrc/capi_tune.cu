@@ -153,8 +153,8 @@ int gb_bfs_autotune(gb_bfs* h, int variant, const uint32_t* sources, int k, gb_b
                     consider(c);
                 }
             c = best;  // then the grid size at the best block / hub cut
-            for (int frac : {4, 2}) {
-                c.grid_blocks = (uint32_t)std::max(1, sms / frac);
+            for (int quarters : {1, 2, 4, 8}) {  // sms/4, sms/2, sms, 2*sms blocks
+                c.grid_blocks = (uint32_t)std::max(1, sms * quarters / 4);
                 consider(c);
             }
         } else {

@@ -165,27 +165,31 @@ __device__ __forceinline__ unsigned warpAppend(bool want, unsigned* counter) {
 // flips exactly when the last block arrives.  The wait is bounded: after
 // spin_limit polls (or once another block has flagged an error) the block
 // records GB timeout in *err and returns false; callers then leave the kernel.
+// gridArriveWait is the part thread 0 of each block runs (the caller brackets
+// it with __syncthreads); on success it returns after an acquire of the
+// other blocks' writes, so thread 0 may read shared counters right away.
+__device__ __forceinline__ bool gridArriveWait(unsigned* bar, unsigned* err, unsigned long long spinLimit,
+                                               unsigned nblocks) {
+    unsigned inc = (blockIdx.x == 0) ? (0x80000000u - (nblocks - 1)) : 1u;
+    __threadfence();
+    unsigned old = atomicAdd(bar, inc);
+    unsigned long long polls = 0;
+    while (((old ^ ldAcquire(bar)) & 0x80000000u) == 0) {
+        if (++polls > spinLimit || ldVolatile(err) != 0) {
+            atomicOr(err, 1u);
+            return false;
+        }
+        if (polls > 64) __nanosleep(64);
+    }
+    __threadfence();
+    return ldVolatile(err) == 0;
+}
+
 __device__ __forceinline__ bool gridBarrierN(unsigned* bar, unsigned* err, unsigned long long spinLimit,
                                              unsigned nblocks) {
     __shared__ int sOk;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned inc = (blockIdx.x == 0) ? (0x80000000u - (nblocks - 1)) : 1u;
-        __threadfence();
-        unsigned old = atomicAdd(bar, inc);
-        unsigned long long polls = 0;
-        int ok = 1;
-        while (((old ^ ldAcquire(bar)) & 0x80000000u) == 0) {
-            if (++polls > spinLimit || ldVolatile(err) != 0) {
-                atomicOr(err, 1u);
-                ok = 0;
-                break;
-            }
-            if (polls > 64) __nanosleep(64);
-        }
-        __threadfence();
-        sOk = ok && ldVolatile(err) == 0;
-    }
+    if (threadIdx.x == 0) sOk = gridArriveWait(bar, err, spinLimit, nblocks);
     __syncthreads();
     return sOk != 0;
 }

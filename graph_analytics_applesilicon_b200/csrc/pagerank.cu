@@ -256,6 +256,22 @@ __global__ void prInit64Kernel(PrArgs a) {
 // Kahan sum of contrib over v's in-list [b, e), lanes of a group of G threads
 // striding it; 16-byte aligned vector loads of col_idx (entries outside
 // [b, e) are masked; the array is padded so the last vector stays in bounds).
+// Adjacency (col_idx) is read once per sweep: load it without allocating in
+// L1, so L1 keeps the contributions that many rows gather (hub-first order
+// puts the most-gathered ones together).
+__device__ __forceinline__ uint4 ldStream4(const uint32_t* p) {
+    uint4 v;
+    asm("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+        : "l"(p));
+    return v;
+}
+__device__ __forceinline__ uint32_t ldStream(const uint32_t* p) {
+    uint32_t v;
+    asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
 template <bool COHERENT>
 __device__ __forceinline__ float ldContrib(const float* p) {
     if (COHERENT) return *reinterpret_cast<const volatile float*>(p);  // rewritten during the sweep
@@ -267,7 +283,7 @@ __device__ __forceinline__ float gatherStrided(const uint32_t* __restrict__ ci, 
                                                uint32_t e, unsigned rank) {
     Kahan k;
     for (uint32_t i = (b & ~3u) + 4 * rank; i < e; i += 4 * G) {
-        const uint4 q = __ldg(reinterpret_cast<const uint4*>(ci + i));
+        const uint4 q = ldStream4(ci + i);
         if (i >= b) k.add(ldContrib<COHERENT>(contrib + q.x));
         if (i + 1 >= b && i + 1 < e) k.add(ldContrib<COHERENT>(contrib + q.y));
         if (i + 2 >= b && i + 2 < e) k.add(ldContrib<COHERENT>(contrib + q.z));
@@ -280,7 +296,7 @@ template <bool COHERENT = false>
 __device__ __forceinline__ float gatherSerial(const uint32_t* __restrict__ ci, const float* contrib, uint32_t b,
                                               uint32_t e) {
     Kahan k;
-    for (uint32_t i = b; i < e; ++i) k.add(ldContrib<COHERENT>(contrib + __ldg(ci + i)));
+    for (uint32_t i = b; i < e; ++i) k.add(ldContrib<COHERENT>(contrib + ldStream(ci + i)));
     return k.sum;
 }
 
@@ -295,8 +311,8 @@ __device__ __forceinline__ float gatherGroup(const uint32_t* __restrict__ ci, co
     const uint32_t step = 4 * G;
     for (uint32_t i = (b & ~3u) + 4 * rank; i < e; i += 2 * step) {
         const uint32_t j = i + step;
-        const uint4 q = __ldg(reinterpret_cast<const uint4*>(ci + i));
-        const uint4 r = j < e ? __ldg(reinterpret_cast<const uint4*>(ci + j)) : make_uint4(0, 0, 0, 0);
+        const uint4 q = ldStream4(ci + i);
+        const uint4 r = j < e ? ldStream4(ci + j) : make_uint4(0, 0, 0, 0);
         const float a0 = (i >= b) ? ldContrib<COHERENT>(contrib + q.x) : 0.f;
         const float a1 = (i + 1 >= b && i + 1 < e) ? ldContrib<COHERENT>(contrib + q.y) : 0.f;
         const float a2 = (i + 2 >= b && i + 2 < e) ? ldContrib<COHERENT>(contrib + q.z) : 0.f;
