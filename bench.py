@@ -247,9 +247,15 @@ def bfs_config_workload(args, world, rank, local):
         bfs.set_selector(sel2, 1)
     o1 = G.BfsOptions(selector="learned" if sel1 is not None else "rule")
     o1 = bfs.autotune("gpu_do_persistent", srcs64[:2], o1)
-    ob = G.BfsOptions(selector="learned" if sel2 is not None else "rule")
-    tuned = bfs.autotune("batch", srcs64, G.BfsOptions(selector=ob.selector))
-    ob.block, ob.hub_min, ob.grid_blocks = tuned.block, tuned.hub_min, tuned.grid_blocks
+    # the batch runs with whichever selector (learned or the alpha/beta rule)
+    # is faster on this graph after tuning block size, hub cut and grid size
+    batch_cands = {}
+    for sel in (("rule", "learned") if sel2 is not None else ("rule",)):
+        ob_ = bfs.autotune("batch", srcs64, G.BfsOptions(selector=sel))
+        bfs.run_batch(srcs64, opts=ob_)
+        bfs.run_batch(srcs64, opts=ob_)
+        batch_cands[sel] = (bfs.lastGpuMs(), ob_)
+    ob = min(batch_cands.values(), key=lambda x: x[0])[1]
     # exactness of the batch against single-source runs (size-independent)
     d64 = bfs.run_batch(srcs64, opts=ob)
     for i in (0, 17, 63):
@@ -289,6 +295,7 @@ def bfs_config_workload(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": batch_t, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64 masks / u32 depths", "data": "synthetic",
             "config": {"workload": args.workload, "n": g.n, "m": g.m, "sources": 64, "batch_selector": ob.selector,
+                       "batch_tuning_ms": {k: round(v[0], 3) for k, v in batch_cands.items()},
                        "tuned_block": ob.block, "tuned_hub_min": ob.hub_min, "tuned_grid_blocks": ob.grid_blocks,
                        "single_tuned": {"block": o1.block, "grid_blocks": o1.grid_blocks, "hub_min": o1.hub_min},
                        "parallelism": f"replicas{world}"},
@@ -371,7 +378,7 @@ def pagerank_workload(args, world, rank, local):
     g = G.gen.chung_lu(args.n, 2.2, 76.0, 307)
     log(f"chung-lu n={g.n} m={g.m} built in {time.time() - t:.1f}s")
     pr = G.GpuPageRank(g.n, g, g, g.degrees())  # undirected: out-CSR = in-CSR
-    o = G.PrOptions(iters=20)
+    o = pr.autotune(G.PrOptions(iters=20))  # degree-class cut points and block size
     pr.run("gpu_pull_f64", o)
     ref = pr.ranks_f64()
     pr.run("gpu_pull_adaptive", o)
@@ -436,7 +443,8 @@ def pagerank_workload(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": total / args.steps, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "chunglu_pr20", "n": g.n, "m": g.m, "variant": "gpu_pull_adaptive",
-                       "iters": 20, "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (in-CSR 947 MB)"},
+                       "iters": 20, "tuned": {"tg": o.tg, "small_max": o.small_max, "large_min": o.large_min},
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (in-CSR 947 MB)"},
             "e2e": {"value": e2e_sum / args.steps / 20, "unit": "ms/iter", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 4 * g.n},
             "gpu_launches": 21 * args.steps,

@@ -28,7 +28,7 @@ BFS_VARIANTS = {"gpu_vertex": 0, "gpu_naive": 1, "gpu_binned": 2, "gpu_edge": 3,
                 "gpu_do_persistent": 5, "hybrid": 5, "batch": 6}
 STRATEGIES = ["td_ept1", "td_ept2", "td_ept4", "td_warp", "bu"]
 PR_VARIANTS = {"gpu_push": 0, "gpu_pull_scalar": 1, "gpu_pull_vector": 2, "gpu_pull_adaptive": 3,
-               "gpu_pull_gs": 4, "gpu_pull_f64": 5}
+               "gpu_pull_gs": 4, "gpu_pull_f64": 5, "gpu_pull_blocked": 6}
 ERRORS = {1: "invalid argument", 2: "CUDA failure", 3: "out of memory", 4: "device wait timed out",
           5: "bad state", 6: "I/O error", 7: "capacity"}
 
@@ -50,7 +50,7 @@ class BfsOptions(C.Structure):
                 ("ept", C.c_uint32), ("alpha", C.c_double), ("beta", C.c_double),
                 ("selector", C.c_uint32), ("force_strategy", C.c_int32), ("hub_min", C.c_uint32),
                 ("block", C.c_uint32), ("spin_limit", C.c_uint64), ("grid_blocks", C.c_uint32),
-                ("pad_", C.c_uint32)]
+                ("sel_margin", C.c_float)]
 
     def __init__(self, **kw):
         super().__init__()

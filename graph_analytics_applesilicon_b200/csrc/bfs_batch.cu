@@ -65,6 +65,7 @@ struct BArgs {
     int k;
     uint32_t hubMin, traceCap;
     double alpha, beta;
+    float selMargin;  // learned selector: log2 margin for leaving the rule's direction
     int selector, force;
     unsigned long long spinLimit;
 };
@@ -349,7 +350,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                 float f[kSelFeatures];
                 selectorFeatures((double)size, (double)fedges, (double)(a.m > fullEdges ? a.m - fullEdges : 0),
                                  (double)(a.n - fullCount), (double)a.n, (double)a.m, (double)level, f);
-                const int s = selectorArgmin(sm.sel, f, tid);
+                const int s = selectorChoose(sm.sel, f, tid, bottomUp, a.selMargin);
                 if (tid == 0) sm.strat = s;
             }
             __syncthreads();
@@ -605,6 +606,7 @@ void gb_bfs::runBatch(const uint32_t* src, int k, const gb_bfs_options& o, std::
     a.hubMin = std::max<uint32_t>(o.hub_min, 32);
     a.traceCap = kTraceCap;
     a.alpha = o.alpha;
+    a.selMargin = o.sel_margin;
     a.beta = o.beta;
     a.selector = (int)o.selector;
     a.force = o.force_strategy;

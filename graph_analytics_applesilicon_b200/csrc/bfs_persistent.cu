@@ -52,6 +52,7 @@ struct PArgs {
     uint64_t n, m;
     uint32_t words, source, hubMin, traceCap;
     double alpha, beta;
+    float selMargin;  // learned selector: log2 margin for leaving the rule's direction
     int selector, force;
     unsigned long long spinLimit;
     uint32_t startLevel, maxLevels;
@@ -442,7 +443,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
                 float f[kSelFeatures];
                 selectorFeatures((double)size, (double)fedges, (double)unexplored, (double)(a.n - reached),
                                  (double)a.n, (double)a.m, (double)level, f);
-                int s = selectorArgmin(sm.sel, f, tid);
+                int s = selectorChoose(sm.sel, f, tid, bottomUp, a.selMargin);
                 if (tid == 0) sm.strat = s;
             }
             __syncthreads();
@@ -605,6 +606,7 @@ PArgs makeArgs(gb_bfs& h, const gb_bfs_options& o, uint32_t src) {
     a.source = src;
     a.hubMin = std::max<uint32_t>(o.hub_min, 32);
     a.alpha = o.alpha;
+    a.selMargin = o.sel_margin;
     a.beta = o.beta;
     a.selector = (int)o.selector;
     a.force = o.force_strategy;
@@ -678,115 +680,43 @@ void gb_bfs::runPersistent(uint32_t src, const gb_bfs_options& o, std::vector<gb
     }
 }
 
-// Selector training data: advance the BFS one level at a time (alpha/beta
-// rule), and before each level time every strategy from the same state
-// (device buffers snapshotted and restored), each a one-level cooperative
-// launch timed inside the kernel between two grid barriers.
+// Selector training data.  A level's vertex set does not depend on the
+// strategy that ran the earlier levels, so running the whole BFS once per
+// strategy (forced at every level, alpha/beta rule off) gives every level's
+// device time under every strategy, measured in a running traversal (warm
+// caches, the real barrier and counter traffic) rather than in a one-level
+// launch.  The features come from the top-down run's trace, whose per-level
+// edge count is the frontier's degree sum, exactly as the kernel sees it.
 size_t gb_bfs::profileLevels(uint32_t src, const gb_bfs_options& o0, int repeats, float* feats, float* times,
                              size_t cap) {
     gb_bfs_options o = o0;
     o.selector = GB_SELECT_RULE;
-    validateOptions(o);
-    ensurePersistent(o);
-    const uint64_t words = (n + 31) / 32;
-    // snapshot buffers
-    DevBuf<uint32_t> sDist, sQ[3], sHub[2], sBm[3], sVis;
-    DevBuf<unsigned long long> sHo;
-    DevBuf<GbPCounters> sCtr;
-    DevBuf<double> sState;
-    sDist.ensure(n);
-    for (auto& b : sQ) b.ensure(n);
-    const uint64_t hubCap = std::min<uint64_t>(n, m / 32 + 1);
-    for (auto& b : sHub) b.ensure(hubCap);
-    sHo.ensure(hubCap);
-    for (auto& b : sBm) b.ensure(words);
-    sVis.ensure(words);
-    sCtr.ensure(3);
-    sState.ensure(S_COUNT);
-    auto copy = [&](void* dst, const void* srcp, size_t bytes) {
-        GB_CUDA(cudaMemcpyAsync(dst, srcp, bytes, cudaMemcpyDeviceToDevice, stream.s));
-    };
-    int qc = 0;
-    auto snapshot = [&](bool save) {
-        auto mv = [&](void* a, void* b, size_t bytes) { save ? copy(a, b, bytes) : copy(b, a, bytes); };
-        mv(sDist.get(), dist.get(), n * 4);
-        for (int j = 0; j < 3; ++j) mv(sQ[j].get(), pq[qc][j].get(), n * 4);
-        for (int j = 0; j < 2; ++j) mv(sHub[j].get(), phub[qc][j].get(), hubCap * 4);
-        mv(sHo.get(), phubOff[qc].get(), hubCap * 8);
-        for (int j = 0; j < 3; ++j) mv(sBm[j].get(), pbm[j].get(), words * 4);
-        mv(sVis.get(), pvisited.get(), words * 4);
-        mv(sCtr.get(), pctr.get(), 3 * sizeof(GbPCounters));
-        mv(sState.get(), pstate.get(), S_COUNT * sizeof(double));
-    };
-    auto run = [&](uint32_t startLevel, uint32_t maxLevels, int force) {
-        PArgs a = makeArgs(*this, o, src);
-        a.startLevel = startLevel;
-        a.maxLevels = maxLevels;
-        a.force = force;
-        a.selector = GB_SELECT_RULE;
-        GB_CUDA(cudaMemsetAsync(pctl.get(), 0, 4 * sizeof(unsigned), stream.s));
-        launchFor(*this, a);
-        unsigned ctl[4];
-        GB_CUDA(cudaMemcpyAsync(ctl, pctl.get(), sizeof ctl, cudaMemcpyDeviceToHost, stream.s));
-        GB_CUDA(cudaStreamSynchronize(stream.s));
-        if (ctl[1]) throw Error(GB_ERR_TIMEOUT, "profiling run: grid barrier timeout");
-        return ctl[2];
-    };
-    // Level 0 has no saved state to restore: each strategy is timed by a
-    // fresh launch (prologue + level 0); later levels restore the snapshot.
-    size_t rows = 0;
-    std::vector<double> st(S_COUNT);
-    std::vector<GbPCounters> ctr(3);
-    for (uint32_t level = 0;; ++level) {
-        if (level == 0) {
-            // Prologue + level 0 with each strategy, from scratch every time.
-            float best[GB_NUM_STRATS];
-            for (int k = 0; k < GB_NUM_STRATS; ++k) {
-                best[k] = 1e30f;
-                for (int r = 0; r < repeats; ++r) {
-                    run(0, 1, k);
-                    gb_level t;
-                    GB_CUDA(cudaMemcpy(&t, ptrace.get(), sizeof t, cudaMemcpyDeviceToHost));
-                    best[k] = std::min(best[k], (float)(t.time_ms * 1e3));
-                }
-            }
-            const uint32_t d0 = degree(src);
-            if (rows < cap) {
-                selectorFeatures(1.0, (double)d0, (double)(m - d0), (double)(n - 1), (double)n, (double)m, 0.0,
-                                 feats + rows * kSelFeatures);
-                for (int k = 0; k < GB_NUM_STRATS; ++k) times[rows * GB_NUM_STRATS + k] = best[k];
-            }
-            ++rows;
-            run(0, 1, -1);  // advance with the rule
-            qc = 1;
-            continue;
-        }
-        GB_CUDA(cudaMemcpy(st.data(), pstate.get(), S_COUNT * sizeof(double), cudaMemcpyDeviceToHost));
-        GB_CUDA(cudaMemcpy(ctr.data(), pctr.get(), 3 * sizeof(GbPCounters), cudaMemcpyDeviceToHost));
-        const GbPCounters& prev = ctr[(level + 2) % 3];
-        if (prev.found == 0) break;
-        qc = (int)(level & 1);
-        snapshot(true);
-        float best[GB_NUM_STRATS];
-        for (int k = 0; k < GB_NUM_STRATS; ++k) {
-            best[k] = 1e30f;
-            for (int r = 0; r < repeats; ++r) {
-                snapshot(false);
-                run(level, 1, k);
-                gb_level t;
-                GB_CUDA(cudaMemcpy(&t, ptrace.get() + std::min<uint32_t>(level, kTraceCap - 1), sizeof t,
-                                   cudaMemcpyDeviceToHost));
-                best[k] = std::min(best[k], (float)(t.time_ms * 1e3));
+    std::vector<std::vector<gb_level>> per(GB_NUM_STRATS);
+    for (int s = 0; s < GB_NUM_STRATS; ++s) {
+        o.force_strategy = s;
+        for (int r = 0; r <= repeats; ++r) {  // run 0 warms up
+            std::vector<gb_level> tr;
+            runPersistent(src, o, &tr);
+            if (r == 0) continue;
+            if (per[s].empty()) {
+                per[s] = tr;
+            } else {
+                for (size_t i = 0; i < std::min(tr.size(), per[s].size()); ++i)
+                    per[s][i].time_ms = std::min(per[s][i].time_ms, tr[i].time_ms);
             }
         }
-        if (rows < cap) {
-            selectorFeatures((double)prev.found, (double)prev.nextEdges, st[S_UNEXPLORED], (double)n - st[S_REACHED],
-                             (double)n, (double)m, (double)level, feats + rows * kSelFeatures);
-            for (int k = 0; k < GB_NUM_STRATS; ++k) times[rows * GB_NUM_STRATS + k] = best[k];
-        }
-        ++rows;
-        snapshot(false);
-        run(level, 1, -1);
+        if (per[s].size() != per[0].size()) throw Error(GB_ERR_STATE, "level count differs between strategies");
     }
-    return std::min(rows, cap);
+    const std::vector<gb_level>& td = per[GB_STRAT_TD_EPT2];
+    double reached = 0, seenEdges = 0;
+    size_t rows = 0;
+    for (size_t L = 0; L < td.size() && rows < cap; ++L, ++rows) {
+        const double frontier = (double)td[L].frontier, fedges = (double)td[L].edges;
+        reached += frontier;
+        seenEdges += fedges;
+        selectorFeatures(frontier, fedges, std::max(0.0, (double)m - seenEdges), std::max(0.0, (double)n - reached),
+                         (double)n, (double)m, (double)L, feats + rows * kSelFeatures);
+        for (int s = 0; s < GB_NUM_STRATS; ++s) times[rows * GB_NUM_STRATS + s] = (float)(per[s][L].time_ms * 1e3);
+    }
+    return rows;
 }

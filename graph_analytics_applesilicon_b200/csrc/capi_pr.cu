@@ -60,7 +60,7 @@ int gb_pr_create(uint64_t n, const uint32_t* out_row_ptr, const uint32_t* out_co
         h->hostOutdeg.assign(outdeg, outdeg + n);
         for (int i = 0; i < 2; ++i) {
             h->r[i].ensure(n + 1);
-            h->contrib[i].ensure(n + 1);
+            h->contrib[i].ensure(n + 4);  // the blocked pull copies whole 16-byte groups past n
         }
         h->ctl.ensure(1);
         h->partF.ensure(2 * 4096);

@@ -185,8 +185,8 @@ int gb_pr_autotune(gb_pr* h, gb_pr_options* o) {
                 best.large_min = c.large_min;
             }
         };
-        for (uint32_t sm : {4u, 8u, 16u, 32u})
-            for (uint32_t lm : {128u, 256u, 1024u, 4096u})
+        for (uint32_t sm : {8u, 16u, 32u, 64u})
+            for (uint32_t lm : {256u, 1024u, 2048u, 4096u, 16384u})
                 for (uint32_t tg : {128u, 256u, 512u}) {
                     c.small_max = sm;
                     c.large_min = lm;

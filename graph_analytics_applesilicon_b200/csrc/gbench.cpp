@@ -10,7 +10,7 @@
 // GPU variants call the B200 library through include/graph_b200.hpp.  New:
 // gpu_do_persistent (and hybrid, which maps to it), --selector rule|learned,
 // --batch 64 (sources in batches of up to 64 per launch), --block, --hub-min,
-// gpu_pull_f64, and the benchmark graphs synth:rmat22, synth:road1400,
+// gpu_pull_f64, gpu_pull_blocked, and the benchmark graphs synth:rmat22, synth:road1400,
 // synth:web875k, synth:chunglu3m.  cpu_serial / cpu_omp / cpu_do are this
 // program's own CPU implementations of the reference's CPU variants
 // (src/cpu/bfs_cpu.cpp, src/cpu/pagerank_cpu.cpp); --validate uses cpu_serial.
@@ -627,7 +627,8 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
 }
 
 const std::vector<std::string> kPrVariants = {"cpu_serial", "cpu_omp", "gpu_push", "gpu_pull_scalar",
-                                              "gpu_pull_vector", "gpu_pull_adaptive", "gpu_pull_gs", "gpu_pull_f64"};
+                                              "gpu_pull_vector", "gpu_pull_adaptive", "gpu_pull_gs", "gpu_pull_f64",
+                                              "gpu_pull_blocked"};
 
 int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
     const std::string variant = args.get("variant", "cpu_serial");

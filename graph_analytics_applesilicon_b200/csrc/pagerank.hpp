@@ -33,7 +33,24 @@ struct GbPrControl {
     float dangHi, dangLo;   // dangling rank of the current iterate (float-float)
     double dang64;          // same, double-precision variant
     double sum64;           // in-place variants: sum of the new iterate
+    int error;              // a bounded device wait gave up (the run is invalid)
 };
+
+// Blocked pull (GB_PR_PULL_BLOCKED): rows in blocks of at most kBlkRowCap
+// (their sums in shared memory), columns in parts of kBlkPart vertices; per
+// part, its contributions and the row block's edge group (a kBlkHdr-word
+// header of per-warp ranges, then the edges) are staged in shared memory by a
+// ring of kBlkStages buffers (groups longer than kBlkEdgeBuf words read the
+// rest from global memory).  kBlkWarps consumer warps own the row block's
+// rows in kBlkWarps contiguous slices.
+constexpr uint32_t kBlkPart = 8192;
+constexpr uint32_t kBlkEdgeBuf = 8192;
+constexpr uint32_t kBlkStages = 2;
+constexpr uint32_t kBlkRowCap = 23000;
+constexpr uint32_t kBlkWarps = 31;
+constexpr uint32_t kBlkHdr = 32;
+constexpr uint32_t kBlkHub = 4096;  // rows with this many in-edges are summed apart, one block each
+constexpr int kBlkThreads = 1024;
 
 struct gb_pr {
     uint64_t n = 0, mOut = 0, mIn = 0;
@@ -88,6 +105,12 @@ struct gb_pr {
     bool gsLastRun = false;
     int lastVariant = -1;
 
+    // blocked pull: packed (row in block << 16 | column in part) per edge,
+    // grouped by row block then part; blkOff[k * nParts + p] starts the group
+    gb::DevBuf<uint32_t> blkEdges, blkOff, blkHubs;
+    uint32_t nRowBlocks = 0, rowsPer = 0, nParts = 0, nBlkHubs = 0;
+    bool blkReady = false;
+
     // cached CUDA graphs of iteration batches
     std::map<std::tuple<int, int, int, int, int, int, int>, cudaGraphExec_t> graphs;
     int grid = 0;
@@ -96,6 +119,7 @@ struct gb_pr {
     void invalidateGraphs();
     void prepareAdaptive(uint32_t smallMax, uint32_t largeMin);
     void prepareGS(uint32_t pairMaxOutdeg);
+    void prepareBlocked();
     gb_pr_result run(int variant, const gb_pr_options& o);
     void ranks(float* out);
     void ranks64(double* out);

@@ -7,6 +7,8 @@
 // :416-420 (kept here as the fallback and as the judge).
 #pragma once
 
+#include <cmath>
+
 #include "common.cuh"
 
 namespace gb {
@@ -17,8 +19,9 @@ constexpr int kSelOutputs = GB_NUM_STRATS;
 constexpr int kSelParams = kSelHidden * kSelFeatures + kSelHidden + kSelHidden * kSelHidden + kSelHidden +
                            kSelOutputs * kSelHidden + kSelOutputs;
 
-// Feature vector of a level (the same on host and device, all inputs exact
-// integers from the level counters):
+// Feature vector of a level (the same function on host and device; inputs
+// are exact integer counters, converted to float first, and only float
+// arithmetic follows, so a device level costs a few instructions per feature):
 //   0 log2(1+frontier vertices)/32   1 log2(1+frontier edges)/32
 //   2 log2(1+unexplored edges)/32    3 log2(1+unvisited vertices)/32
 //   4 log2(1+n)/32                   5 log2(1+m)/32
@@ -26,14 +29,15 @@ constexpr int kSelParams = kSelHidden * kSelFeatures + kSelHidden + kSelHidden *
 __host__ __device__ inline void selectorFeatures(double frontier, double fedges, double unexplored,
                                                  double unvisited, double n, double m, double level,
                                                  float* f) {
-    f[0] = (float)(log2(1.0 + frontier) / 32.0);
-    f[1] = (float)(log2(1.0 + fedges) / 32.0);
-    f[2] = (float)(log2(1.0 + unexplored) / 32.0);
-    f[3] = (float)(log2(1.0 + unvisited) / 32.0);
-    f[4] = (float)(log2(1.0 + n) / 32.0);
-    f[5] = (float)(log2(1.0 + m) / 32.0);
-    f[6] = (float)((level < 255.0 ? level : 255.0) / 256.0);
-    f[7] = (float)(log2(1.0 + fedges / (frontier > 1.0 ? frontier : 1.0)) / 16.0);
+    const float fr = (float)frontier, fe = (float)fedges;
+    f[0] = log2f(1.0f + fr) * (1.0f / 32.0f);
+    f[1] = log2f(1.0f + fe) * (1.0f / 32.0f);
+    f[2] = log2f(1.0f + (float)unexplored) * (1.0f / 32.0f);
+    f[3] = log2f(1.0f + (float)unvisited) * (1.0f / 32.0f);
+    f[4] = log2f(1.0f + (float)n) * (1.0f / 32.0f);
+    f[5] = log2f(1.0f + (float)m) * (1.0f / 32.0f);
+    f[6] = (level < 255.0 ? (float)level : 255.0f) * (1.0f / 256.0f);
+    f[7] = log2f(1.0f + fe / (fr > 1.0f ? fr : 1.0f)) * (1.0f / 16.0f);
 }
 
 #ifdef __CUDACC__
@@ -60,12 +64,15 @@ __device__ __forceinline__ void selectorStage(float* S, const float* P, unsigned
     }
 }
 
-// One warp evaluates the MLP (lane j owns hidden unit j) and returns the
-// strategy with the smallest predicted time, or -1 if an output is not finite.
+// One warp evaluates the MLP (lane j owns hidden unit j) on the features of
+// a level and returns the strategy to run, or -1 if an output is not finite.
+// ruleBU is the alpha/beta rule's direction; with margin 0 the result is the
+// strategy of smallest predicted time.
 // S is the shared-memory copy written by selectorStage.  Every lane returns
 // the same value; the result depends only on the parameters and f, so every
 // block of a grid that calls it on the same counters agrees.
-__device__ __forceinline__ int selectorArgmin(const float* S, const float* f, unsigned lane) {
+__device__ __forceinline__ int selectorChoose(const float* S, const float* f, unsigned lane, bool ruleBU,
+                                              float margin) {
     const float* w1 = S;  // [k][j]
     const float* b1 = w1 + kSelHidden * kSelFeatures;
     const float* w2 = b1 + kSelHidden;  // [k][j]
@@ -84,8 +91,11 @@ __device__ __forceinline__ int selectorArgmin(const float* S, const float* f, un
     float out = b3[o];
 #pragma unroll
     for (int k = 0; k < kSelHidden; ++k) out = fmaf(w3[k * kSelOutputs + o], __shfl_sync(kFull, h2, k), out);
-    bool bad = lane < kSelOutputs && !isfinite(out);
-    float key = lane < kSelOutputs ? out : 3.0e38f;
+    if (__any_sync(kFull, lane < kSelOutputs && !isfinite(out))) return -1;
+    // the fastest top-down strategy (GB_STRAT_TD_EPT1..TD_WARP = 0..3), then
+    // the direction: the rule's unless the other one is predicted faster by
+    // more than `margin` (log2 time)
+    float key = lane < GB_STRAT_BU ? out : 3.0e38f;
     int idx = (int)lane;
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) {
@@ -96,7 +106,9 @@ __device__ __forceinline__ int selectorArgmin(const float* S, const float* f, un
             idx = i2;
         }
     }
-    return __any_sync(kFull, bad) ? -1 : idx;
+    const float tBU = __shfl_sync(kFull, out, GB_STRAT_BU);
+    if (ruleBU) return key + margin < tBU ? idx : GB_STRAT_BU;
+    return tBU + margin < key ? GB_STRAT_BU : idx;
 }
 #endif
 

@@ -38,7 +38,7 @@ def training_graphs():
     for scale, ef, seed in ((16, 16, 101), (18, 8, 102), (18, 32, 103), (20, 4, 104), (20, 16, 105), (21, 8, 106)):
         g = G.gen.rmat(scale, ef, False, seed)
         out.append((f"rmat{scale}_ef{ef}", G.permute(g, G.random_perm(g.n, seed))))
-    for rows, seed in ((300, 201), (700, 202)):
+    for rows, seed in ((300, 201), (700, 202), (1000, 203)):
         out.append((f"road{rows}", G.gen.road(rows, rows, 0.04, 0.005, seed)))
     for n, deg, seed in ((200000, 20.0, 301), (500000, 60.0, 302)):
         out.append((f"chunglu{n}_{int(deg)}", G.gen.chung_lu(n, 2.2, deg, seed)))
@@ -60,7 +60,7 @@ def heldout_graphs():
 def generate_batch(path, batches_per_graph=2, repeats=2, max_rows_per_batch=400):
     """Rows for the 64-source batched kernel (each strategy forced for the whole
     batch; every level's time is read from the device trace)."""
-    feats, times = [], []
+    feats, times, tags = [], [], []
     for name, g in training_graphs():
         t0 = time.time()
         bfs = G.GpuBfs(g)
@@ -72,9 +72,10 @@ def generate_batch(path, batches_per_graph=2, repeats=2, max_rows_per_batch=400)
                 f, t = f[keep], t[keep]
             feats.append(f)
             times.append(t)
+            tags += [name] * len(f)
         bfs.close()
         print(f"{name}: rows so far {sum(len(x) for x in feats)} ({time.time() - t0:.1f}s)", flush=True)
-    np.savez_compressed(path, feats=np.concatenate(feats), times=np.concatenate(times))
+    np.savez_compressed(path, feats=np.concatenate(feats), times=np.concatenate(times), tags=np.array(tags))
 
 
 def save_params(p, out_path):
@@ -118,6 +119,13 @@ def train(data_path, out_path=None, epochs=600, batch=128, lr=3e-3, seed=0):
     y = np.log2(t).astype(np.float32)
     mask = np.isfinite(y).astype(np.float32) * (d["times"] < 1e20)
     y = np.where(mask > 0, y, 0).astype(np.float32)
+    if "tags" in d.files:
+        # every training graph weighs the same: a long-diameter graph gives
+        # hundreds of levels, a power-law graph a dozen
+        tags = d["tags"]
+        names, inv, counts = np.unique(tags, return_inverse=True, return_counts=True)
+        w = (len(tags) / len(names)) / counts[inv]
+        mask = mask * w[:, None].astype(np.float32)
     p = init_params(seed)
     loss = G.C.c_float(0)
     G.check(G.lib().gb_mlp_train(p, len(x), np.ascontiguousarray(x), np.ascontiguousarray(y),

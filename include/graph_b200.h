@@ -131,7 +131,11 @@ typedef struct {
     uint32_t block;      /* persistent / batched: threads per block (256 or 512) */
     uint64_t spin_limit; /* grid-barrier wait bound in polls (0 = default, ~ seconds) */
     uint32_t grid_blocks; /* persistent / batched: blocks in the grid (0 = every resident block) */
-    uint32_t pad_;
+    float sel_margin;    /* learned selector: it departs from the alpha/beta rule's direction only
+                            when it predicts the other direction faster by this much (log2 of
+                            the time ratio); its top-down strategy choice is free.  0 = pure
+                            argmin.  A direction change costs work the per-level predictions do
+                            not see (a bottom-up to top-down switch rebuilds the queue). */
 } gb_bfs_options;
 
 void gb_bfs_default_options(gb_bfs_options* o);
@@ -186,9 +190,10 @@ int gb_mlp_loss_grad(const float* params, int batch, const float* x, const float
 int gb_mlp_forward(const float* params, int batch, const float* x, float* out);
 int gb_mlp_train(float* params_inout, int rows, const float* x, const float* y, const float* mask,
                  int epochs, int batch, float lr, uint64_t seed, float* final_loss);
-/* Training data: run a single-source BFS level by level; at every level run
- * each strategy from the same state, time it on the device, and record the
- * level's features (gb_selector_shape) and the per-strategy times (us).
+/* Training data: run the single-source persistent BFS once per strategy, the
+ * strategy forced at every level (a level's vertex set does not depend on it),
+ * and record each level's features (gb_selector_shape) and its device time
+ * under every strategy (us, min over `repeats` runs after a warm-up run).
  * rows_out: [cap][n_features] features, times_out: [cap][GB_NUM_STRATS].
  * Returns the number of rows via *rows. */
 int gb_bfs_profile_levels(gb_bfs* h, uint32_t source, const gb_bfs_options* opt, int repeats,
@@ -211,7 +216,11 @@ typedef enum {
     GB_PR_PULL_VECTOR = 2,   /* gpu_pull_vector   (:317-327) */
     GB_PR_PULL_ADAPTIVE = 3, /* gpu_pull_adaptive (:338-381) */
     GB_PR_PULL_GS = 4,       /* gpu_pull_gs       (src/metal/pagerank_gpu.mm:88-192) */
-    GB_PR_PULL_F64 = 5       /* double-precision Jacobi pull: the GPU oracle for FP32 runs */
+    GB_PR_PULL_F64 = 5,      /* double-precision Jacobi pull: the GPU oracle for FP32 runs */
+    GB_PR_PULL_BLOCKED = 6   /* gpu_pull_blocked: Jacobi pull with the contributions staged in
+                                shared memory, one 16K-vertex part at a time (TMA bulk copies),
+                                over a per-row-block, per-part edge list; no reference counterpart
+                                (a B200 layout of gpu_pull_*, src/metal/pagerank_gpu.mm:276-297) */
 } gb_pr_variant;
 
 /* GpuPrOptions (src/metal/pagerank_gpu.hpp:27-36). */

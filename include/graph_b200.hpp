@@ -92,7 +92,8 @@ private:
 
 // PrVariant / parsePrVariant (src/metal/pagerank_gpu.hpp:25, pagerank_gpu.mm:21-28).
 enum class PrVariant { Push = GB_PR_PUSH, PullScalar = GB_PR_PULL_SCALAR, PullVector = GB_PR_PULL_VECTOR,
-                       PullAdaptive = GB_PR_PULL_ADAPTIVE, PullGS = GB_PR_PULL_GS, PullF64 = GB_PR_PULL_F64 };
+                       PullAdaptive = GB_PR_PULL_ADAPTIVE, PullGS = GB_PR_PULL_GS, PullF64 = GB_PR_PULL_F64,
+                       PullBlocked = GB_PR_PULL_BLOCKED };
 
 inline PrVariant parsePrVariant(const std::string& s) {
     if (s == "gpu_push") return PrVariant::Push;
@@ -101,6 +102,7 @@ inline PrVariant parsePrVariant(const std::string& s) {
     if (s == "gpu_pull_adaptive") return PrVariant::PullAdaptive;
     if (s == "gpu_pull_gs") return PrVariant::PullGS;
     if (s == "gpu_pull_f64") return PrVariant::PullF64;
+    if (s == "gpu_pull_blocked") return PrVariant::PullBlocked;
     throw std::runtime_error("unknown GPU PageRank variant '" + s + "'");
 }
 

@@ -9,6 +9,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 CFGS = [("gpu_push", 16, 256), ("gpu_pull_scalar", 16, 256), ("gpu_pull_vector", 16, 256),
+        ("gpu_pull_blocked", 16, 256),
         ("gpu_pull_adaptive", 16, 256), ("gpu_pull_adaptive", 1 << 30, 1 << 31),
         ("gpu_pull_adaptive", 0, 0), ("gpu_pull_adaptive", 0, 1 << 30), ("gpu_pull_adaptive", 2, 3)]
 
@@ -128,7 +129,7 @@ def test_larger_graphs_fp32_vs_fp64(gb, oracle):
         h.run("gpu_pull_f64", gb.PrOptions(tol=tol, iters=iters))
         r64 = h.ranks_f64()
         assert np.abs(r64 - ref).sum() < 1e-10
-        for variant in ("gpu_pull_adaptive", "gpu_pull_vector", "gpu_pull_scalar", "gpu_push"):
+        for variant in ("gpu_pull_adaptive", "gpu_pull_blocked", "gpu_pull_vector", "gpu_pull_scalar", "gpu_push"):
             r = h.run(variant, gb.PrOptions(tol=tol, iters=iters))
             c = oracle.check_ranks(r64, h.ranks())
             assert c.ok() and c.l1 < 1e-5, (variant, tol, c)
@@ -160,3 +161,25 @@ def test_gs_with_split_hubs(gb, oracle):
             h.run("gpu_pull_gs", gb.PrOptions(tol=2.5e-7, iters=1000))
             assert oracle.gs_no_worse(oracle.check_ranks(conv, h.ranks()), jerr), (g.n, K)
     assert True in modes
+
+
+def test_blocked_pull_layouts(gb, oracle):
+    """gpu_pull_blocked against the FP64 GPU pull and the CPU oracle on graphs
+    that exercise its layout: many column parts and row blocks with split-off
+    rows of >= 4096 in-edges (web-shaped, Chung-Lu), a last part that is not a
+    multiple of 4 vertices, and more row blocks than SMs (a 4M-vertex path,
+    so blocks loop over several row blocks)."""
+    cases = [gb.gen.web(200003, 5.8, 2.1, 17), gb.gen.chung_lu(300001, 2.2, 40.0, 5), gb.gen.path(4000001)]
+    for g in cases:
+        gin = gb.transpose(g) if g.directed else g
+        od = g.degrees()
+        h = gb.GpuPageRank(g.n, None, gin, od)
+        for tol, iters in ((0.0, 20), (1e-6, 1000)):
+            ref, ref_iters, _ = oracle.pagerank_serial(gin, od, iters, tol)
+            r = h.run("gpu_pull_blocked", gb.PrOptions(tol=tol, iters=iters))
+            c = oracle.check_ranks(ref, h.ranks())
+            assert c.ok() and c.l1 < 1e-5, (g.n, tol, c)
+            if tol == 0:
+                assert r.iters == 20
+            elif not r.floor_stop:
+                assert abs(r.iters - ref_iters) <= 3, (g.n, r.iters, ref_iters)

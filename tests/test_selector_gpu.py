@@ -52,7 +52,8 @@ def test_gpu_training_fits_a_known_function(gb):
 
 def test_selector_picks_never_change_depths(gb, oracle):
     """Random selector parameters (arbitrary strategy sequences) and the
-    shipped ones give cpu_serial's depths."""
+    shipped ones give cpu_serial's depths; with an unbounded direction margin
+    the directions are the alpha/beta rule's."""
     nf, nh, no = shape(gb)
     rng = np.random.default_rng(3)
     graphs = [gb.gen.rmat(15, 16, False, 7), gb.gen.road(150, 150, 0.04, 0.005, 8), gb.gen.star(50000)]
@@ -67,9 +68,13 @@ def test_selector_picks_never_change_depths(gb, oracle):
             _, ctr = oracle.bfs_do(g, int(s))
             for p in params:
                 bfs.set_selector(p, 0)
-                d, tr = bfs.run("gpu_do_persistent", int(s), opts=gb.BfsOptions(selector="learned"), trace=True)
-                assert np.array_equal(d, ref)
-                assert [L["frontier"] for L in tr] == [t[2] for t in ctr]
+                for margin in (0.0, 0.5, 1e9):
+                    o = gb.BfsOptions(selector="learned", sel_margin=margin)
+                    d, tr = bfs.run("gpu_do_persistent", int(s), opts=o, trace=True)
+                    assert np.array_equal(d, ref)
+                    assert [L["frontier"] for L in tr] == [t[2] for t in ctr]
+                    if margin > 1e6:  # direction left to the alpha/beta rule
+                        assert [L["direction"] for L in tr] == [t[1] for t in ctr]
 
 
 def test_learned_without_parameters_is_an_error(gb):
