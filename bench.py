@@ -176,6 +176,20 @@ def cpu_baseline(g, srcs, budget_s=15.0):
             "sample": f"cpu_do alpha=15 beta=18 from {used} of the {len(srcs)} sources, {secs:.1f}s"}
 
 
+def measured_traffic(kernel, workload):
+    """DRAM bytes (read + write) per launch of `kernel` on `workload`, as measured by ncu
+    and recorded in profiles/roofline_traffic.txt (None if not recorded)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and parts[1] == workload:
+                    return int(parts[2])
+    except OSError:
+        pass
+    return None
+
+
 def init_dist(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -449,7 +463,8 @@ def pagerank_workload(args, world, rank, local):
                     "d2h_bytes_per_step": 4 * g.n},
             "gpu_launches": 21 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_source": peak_kind, "kernel": "prPullKernel<2,false>",
+                         "traffic": measured_traffic("prPullKernel<2>", "chunglu_pr20") if args.n == 3070000 else None,
+                         "peak_source": peak_kind, "kernel": "prPullKernel<2,false>",
                          "bytes_per_launch": bytes_sweep, "mean_launch_ms": kernel_ms},
             "cpu_baseline": cpu, "clocks": clocks.summary(),
             "accuracy": {"l1_vs_fp64_gpu": l1, "ok": l1 < 1e-4}, "compare": compare}
@@ -561,9 +576,13 @@ def main():
 
     # comparison forms on the same sources (not part of the timed region)
     plain_ms = rule_ms = float("nan")
+    rule_opts = None
     if not args.no_compare:
         plain_ms = device_step("gpu_do", G.BfsOptions())[0]
-        rule_ms = device_step("gpu_do_persistent", G.BfsOptions(selector="rule"))[0]
+        # the alpha/beta rule in the same kernel, tuned the same way
+        rule_opts = bfs.autotune("gpu_do_persistent", srcs[:4], G.BfsOptions(selector="rule"))
+        device_step("gpu_do_persistent", rule_opts)
+        rule_ms = device_step("gpu_do_persistent", rule_opts)[0]
     # reference summary: harmonic mean over sources of per-source GTEPS (src/bench/main.cpp:366-370)
     hmean = len(srcs) / sum((lm * 1e-3) / (c / 1e9) for lm, c in zip(launch_ms[: len(srcs)], comp) if c)
 
@@ -571,13 +590,7 @@ def main():
     bytes_per_trav = 4 * (g.n + 1) + 4 * g.m + 4 * g.n
     mean_launch = statistics.mean(launch_ms)
     achieved = bytes_per_trav / (mean_launch * 1e-3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "persistent_bfs_rmat22_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get("bytes_per_launch")
-        except Exception:
-            traffic = None
+    traffic = measured_traffic("persistentBfsKernel", "rmat22_bfs64") if args.scale == SCALE else None
 
     value = world * edges_per_step * args.steps / (total_ms * 1e-3) / 1e9
     e2e_value = world * edges_per_step * args.steps / (e2e_total * 1e-3) / 1e9
@@ -602,13 +615,16 @@ def main():
         "gpu_launches": len(srcs) * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": "persistentBfsKernel<512>", "bytes_per_launch": bytes_per_trav,
+                     "kernel": f"persistentBfsKernel<{opts.block or 512}>", "bytes_per_launch": bytes_per_trav,
                      "mean_launch_ms": mean_launch},
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
         "validated": bool(valid),
         "compare": {"plain_gpu_do_gteps": edges_per_step / (plain_ms * 1e-3) / 1e9,
                     "persistent_rule_gteps": edges_per_step / (rule_ms * 1e-3) / 1e9,
+                    "persistent_rule_tuned": ({"block": rule_opts.block, "grid_blocks": rule_opts.grid_blocks,
+                                               "hub_min": rule_opts.hub_min} if rule_opts is not None else None),
+                    "speedup_learned_vs_rule": rule_ms / (total_ms / args.steps),
                     "speedup_vs_plain_gpu_do": plain_ms / (total_ms / args.steps),
                     "hmean_gteps_per_source": hmean},
     }
