@@ -412,6 +412,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
     }
     const uint32_t endLevel = a.maxLevels ? a.startLevel + a.maxLevels : 0xFFFFFFFFu;
     uint64_t tPrev = globaltimer();
+    int selLast = -1;  // last evaluated learned decision and the frontier it was made for
+    bool selLastBU = false;
+    float selLastF = 0.0f, selLastE = 0.0f;
     // The previous level's counters, read once after each barrier and carried
     // into the next level in registers.
     uint64_t nextSize, nextEdgesC, nextQ;
@@ -435,43 +438,58 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
         if (!bottomUp && (double)scout > (double)toCheck / a.alpha) bottomUp = true;
         if (!bottomUp) toCheck -= min(toCheck, scout);
         const int ruleStrat = bottomUp ? GB_STRAT_BU : GB_STRAT_TD_EPT2;
-        int strat = ruleStrat;
-        if (a.force >= 0) {
-            strat = a.force;
-        } else if (learned) {
-            if (tid < 32) {
-                float f[kSelFeatures];
-                selectorFeatures((double)size, (double)fedges, (double)unexplored, (double)(a.n - reached),
-                                 (double)a.n, (double)a.m, (double)level, f);
-                int s = selectorChoose(sm.sel, f, tid, bottomUp, a.selMargin);
-                if (tid == 0) sm.strat = s;
+        int strat = a.force >= 0 ? a.force : ruleStrat;
+        // Warp 0 evaluates the learned selector while the other warps do the
+        // level's bookkeeping; one block barrier covers both.  A level whose
+        // frontier differs from the last evaluated one by less than 0.25 in
+        // log2 of both its vertex and edge counts, in the same rule
+        // direction, reuses that decision (every block sees the same
+        // counters, so all blocks reuse alike): long runs of similar levels
+        // (a road graph's 1,800) then skip the evaluation.
+        bool useSel = a.force < 0 && learned;
+        if (useSel) {
+            const float lf = log2f(1.0f + (float)size), le = log2f(1.0f + (float)fedges);
+            if (selLast >= 0 && bottomUp == selLastBU && fabsf(lf - selLastF) < 0.25f && fabsf(le - selLastE) < 0.25f) {
+                strat = selLast;
+                useSel = false;
+            } else {
+                selLastF = lf;
+                selLastE = le;
+                selLastBU = bottomUp;
             }
-            __syncthreads();
-            if (sm.strat >= 0) strat = sm.strat;
         }
-        if (tid == 0) {
-            sm.acc[0] = sm.acc[1] = sm.acc[2] = 0;
+        if (useSel && tid < 32) {
+            float f[kSelFeatures];
+            selectorFeatures((double)size, (double)fedges, (double)unexplored, (double)(a.n - reached), (double)a.n,
+                             (double)a.m, (double)level, f);
+            int s = selectorChoose(sm.sel, f, tid, bottomUp, a.selMargin);
+            if (tid == 0) sm.strat = s;
         }
+        if (tid == 0) sm.acc[0] = sm.acc[1] = sm.acc[2] = 0;
         if (gtid == 0) {
             if (a.trace && level > 0 && level - 1 < a.traceCap && lastStrat == GB_STRAT_BU)
                 a.trace[level - 1].edges = ldv(&prev->examined);
-            if (a.trace && level < a.traceCap) {
-                gb_level r;
-                r.level = level;
-                r.direction = strat == GB_STRAT_BU ? 'B' : 'T';
-                r.device = 'G';
-                r.strategy = (uint8_t)strat;
-                r.pad = (uint8_t)ruleStrat;
-                r.frontier = size;
-                r.edges = fedges;
-                r.time_ms = 0;
-                a.trace[level] = r;
-            }
             a.ctr[(level + 1) % 3] = GbPCounters{};
         }
         uint32_t* clearBm = a.bm[(level + 2) % 3];
         for (uint64_t w = gtid; w < a.words; w += gthreads) clearBm[w] = 0;
         __syncthreads();
+        if (useSel) {
+            if (sm.strat >= 0) strat = sm.strat;
+            selLast = sm.strat;
+        }
+        if (gtid == 0 && a.trace && level < a.traceCap) {
+            gb_level r;
+            r.level = level;
+            r.direction = strat == GB_STRAT_BU ? 'B' : 'T';
+            r.device = 'G';
+            r.strategy = (uint8_t)strat;
+            r.pad = (uint8_t)ruleStrat;
+            r.frontier = size;
+            r.edges = fedges;
+            r.time_ms = 0;
+            a.trace[level] = r;
+        }
 
         Acc acc;
         if (strat == GB_STRAT_BU) {

@@ -749,14 +749,19 @@ __global__ void __launch_bounds__(kBlkThreads, 1) prBlockedKernel(PrArgs a, BlkA
                     const bool real = q != 0xFFFFFFFFu;
                     const uint32_t row = real ? (q >> 16) : 0x10000u + lane;  // padding: a run of its own
                     float val = real ? cbuf[q & 0xFFFFu] : 0.0f;
-#pragma unroll
-                    for (int d = 1; d < 32; d <<= 1) {  // sums of equal-row runs (rows ascend along the lanes)
-                        const float v2 = __shfl_up_sync(kFull, val, d);
-                        const uint32_t r2 = __shfl_up_sync(kFull, row, d);
-                        if ((int)lane >= d && r2 == row) val += v2;
-                    }
                     const uint32_t nextRow = __shfl_down_sync(kFull, row, 1);
-                    if (real && (lane == 31 || nextRow != row)) sums[row] += val;
+                    const bool runEnd = lane == 31 || nextRow != row;
+                    if (__all_sync(kFull, runEnd)) {  // usual case: every lane is its own run
+                        if (real) sums[row] += val;
+                    } else {
+#pragma unroll
+                        for (int d = 1; d < 32; d <<= 1) {  // sums of equal-row runs (rows ascend along the lanes)
+                            const float v2 = __shfl_up_sync(kFull, val, d);
+                            const uint32_t r2 = __shfl_up_sync(kFull, row, d);
+                            if ((int)lane >= d && r2 == row) val += v2;
+                        }
+                        if (real && runEnd) sums[row] += val;
+                    }
                     __syncwarp();
                 }
                 if (lane == 0)

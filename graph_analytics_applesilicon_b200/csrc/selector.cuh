@@ -83,14 +83,16 @@ __device__ __forceinline__ int selectorChoose(const float* S, const float* f, un
 #pragma unroll
     for (int k = 0; k < kSelFeatures; ++k) h1 = fmaf(w1[k * kSelHidden + lane], f[k], h1);
     h1 = fmaxf(h1, 0.0f);
-    float h2 = b2[lane];
+    // 32-term dot products in four independent partial sums (shorter dependency chains)
+    float p2[4] = {b2[lane], 0.0f, 0.0f, 0.0f};
 #pragma unroll
-    for (int k = 0; k < kSelHidden; ++k) h2 = fmaf(w2[k * kSelHidden + lane], __shfl_sync(kFull, h1, k), h2);
-    h2 = fmaxf(h2, 0.0f);
+    for (int k = 0; k < kSelHidden; ++k) p2[k & 3] = fmaf(w2[k * kSelHidden + lane], __shfl_sync(kFull, h1, k), p2[k & 3]);
+    const float h2 = fmaxf((p2[0] + p2[1]) + (p2[2] + p2[3]), 0.0f);
     const unsigned o = lane < kSelOutputs ? lane : 0;
-    float out = b3[o];
+    float p3[4] = {b3[o], 0.0f, 0.0f, 0.0f};
 #pragma unroll
-    for (int k = 0; k < kSelHidden; ++k) out = fmaf(w3[k * kSelOutputs + o], __shfl_sync(kFull, h2, k), out);
+    for (int k = 0; k < kSelHidden; ++k) p3[k & 3] = fmaf(w3[k * kSelOutputs + o], __shfl_sync(kFull, h2, k), p3[k & 3]);
+    const float out = (p3[0] + p3[1]) + (p3[2] + p3[3]);
     if (__any_sync(kFull, lane < kSelOutputs && !isfinite(out))) return -1;
     // the fastest top-down strategy (GB_STRAT_TD_EPT1..TD_WARP = 0..3), then
     // the direction: the rule's unless the other one is predicted faster by
