@@ -176,6 +176,21 @@ def cpu_baseline(g, srcs, budget_s=15.0):
             "sample": f"cpu_do alpha=15 beta=18 from {used} of the {len(srcs)} sources, {secs:.1f}s"}
 
 
+def max_over_ranks(vals, world):
+    """Element-wise maximum of `vals` over all ranks (the slowest rank's times): every
+    multi-GPU figure is the whole job's work over the slowest rank's device time.  Works
+    with the NCCL process group of a GPU run and with gloo (CPU tests)."""
+    vals = [float(v) for v in vals]
+    if world <= 1:
+        return vals
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def measured_traffic(kernel, workload):
     """DRAM bytes (read + write) per launch of `kernel` on `workload`, as measured by ncu
     and recorded in profiles/roofline_traffic.txt (None if not recorded)."""
@@ -295,13 +310,13 @@ def bfs_config_workload(args, world, rank, local):
         bfs.run("gpu_do", int(s))
         plain_ms.append(bfs.lastGpuMs())
     plain_e2e = [_timed(lambda: bfs.run("gpu_do", int(s))) for s in plain[:2]]
+    batch_t, e2e = max_over_ranks([statistics.median(batch_ms), e2e], world)
     if rank != 0:
         return
     e64 = sum(comp.values())
-    batch_t = statistics.median(batch_ms)
     single_gteps = sum(comp[int(s)] for s in single) / (sum(single_ms) * 1e-3) / 1e9
     plain_gteps = sum(comp[int(s)] for s in plain) / (sum(plain_ms) * 1e-3) / 1e9
-    value = e64 / (batch_t * 1e-3) / 1e9
+    value = world * e64 / (batch_t * 1e-3) / 1e9  # every rank runs its own batch (replicas)
     peak, peak_kind = peaks()
     bytes_per_trav = 4 * (g.n + 1) + 4 * g.m + 4 * g.n
     achieved = 64 * bytes_per_trav / (batch_t * 1e-3) / 1e9
@@ -313,7 +328,7 @@ def bfs_config_workload(args, world, rank, local):
                        "tuned_block": ob.block, "tuned_hub_min": ob.hub_min, "tuned_grid_blocks": ob.grid_blocks,
                        "single_tuned": {"block": o1.block, "grid_blocks": o1.grid_blocks, "hub_min": o1.hub_min},
                        "parallelism": f"replicas{world}"},
-            "e2e": {"value": e64 / (e2e * 1e-3) / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 256,
+            "e2e": {"value": world * e64 / (e2e * 1e-3) / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 256,
                     "d2h_bytes_per_step": 4 * 64 * g.n},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -367,6 +382,7 @@ def pagerank_tol_workload(args, world, rank, local):
     gs_ok = res["gpu_pull_gs"]["l1_vs_converged"] <= max(1e-4, jac_l1)
     best = "gpu_pull_gs" if gs_ok and res["gpu_pull_gs"]["ms_to_tol"] < res["gpu_pull_adaptive"]["ms_to_tol"] \
         else "gpu_pull_adaptive"
+    res[best]["ms_to_tol"] = max_over_ranks([res[best]["ms_to_tol"]], world)[0]  # the slowest replica
     if rank != 0:
         return
     out = torch.empty(g.n, dtype=torch.float32, pin_memory=True).numpy()
@@ -421,13 +437,7 @@ def pagerank_workload(args, world, rank, local):
             pr.run("gpu_pull_adaptive", o)
             G.check(G.lib().gb_pr_ranks(pr._h, out))
             e2e.append((time.perf_counter() - t0) * 1e3)
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([total, sum(e2e)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total, e2e_sum = tt.tolist()
-    else:
-        e2e_sum = sum(e2e)
+    total, e2e_sum = max_over_ranks([total, sum(e2e)], world)
     compare = {}
     for v in ("gpu_pull_vector", "gpu_pull_scalar", "gpu_push"):
         rr = [pr.run(v, o).gpu_ms for _ in range(2)]
@@ -568,11 +578,7 @@ def main():
         barrier()
     total_ms = sum(step_ms)
     e2e_total = sum(e2e_ms)
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([total_ms, e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms, e2e_total = tt.tolist()
+    total_ms, e2e_total = max_over_ranks([total_ms, e2e_total], world)
 
     # comparison forms on the same sources (not part of the timed region)
     plain_ms = rule_ms = float("nan")
