@@ -182,14 +182,27 @@ __device__ void tdTile(const PArgs& a, Smem<NT>& sm, uint32_t item, uint32_t S, 
     __syncthreads();
 }
 
-// Warp per queue entry (degree-binned form): lanes stride the adjacency list.
-__device__ __forceinline__ void tdWarpEntry(const PArgs& a, uint32_t idx, uint32_t qc, uint32_t level,
-                                            GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre) {
-    const uint32_t st = a.qs[qc][idx], d = a.qd[qc][idx];
-    for (uint32_t base = 0; base < d; base += 32) {
-        const uint32_t e = base + laneId();
-        const bool has = e < d;
-        discover(a, has, has ? a.col_idx[st + e] : 0u, level, cur, bmNext, qc ^ 1u, acc, pre);
+// Top-down over the queue in groups of G lanes per entry (G = 4..32, a power
+// of two of at least twice the level's mean degree; G = 32 is warp per
+// vertex, the degree-binned form): a warp takes 32/G consecutive entries, and
+// each group strides its vertex's adjacency list.  Low-degree frontiers (road
+// graphs, degree ~4, G = 8) thus use a quarter of the warps, so a quarter of
+// the queue appends, and most vertices still finish in one round.
+__device__ __forceinline__ void tdGroups(const PArgs& a, uint32_t S, unsigned G, uint32_t qc, uint32_t level,
+                                         GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre) {
+    const unsigned lane = laneId(), per = 32u / G;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t base = warp * per; base < S; base += nwarps * per) {  // warp-uniform
+        const uint64_t idx = base + lane / G;
+        const bool has = idx < S;
+        const uint32_t st = has ? a.qs[qc][idx] : 0u, d = has ? a.qd[qc][idx] : 0u;
+        const uint32_t maxd = __reduce_max_sync(kFull, d);
+        for (uint32_t e0 = 0; e0 < maxd; e0 += G) {
+            const uint32_t e = e0 + (lane & (G - 1));
+            const bool he = e < d;
+            discover(a, he, he ? a.col_idx[st + e] : 0u, level, cur, bmNext, qc ^ 1u, acc, pre);
+        }
     }
 }
 
@@ -510,9 +523,11 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
             // tickets, no block barriers); edge-balanced tiles: block tickets
             const bool warpMode = strat == GB_STRAT_TD_WARP;
             if (warpMode) {
-                const uint64_t nwarps = gthreads >> 5;
-                for (uint64_t idx = gtid >> 5; idx < S; idx += nwarps)
-                    tdWarpEntry(a, (uint32_t)idx, qc, level, cur, a.bm[(level + 1) % 3], acc, fedges >= 65536);
+                const uint64_t qEdges = fedges > HE ? fedges - HE : 0;  // the queue entries' edges
+                // group of at least twice the mean degree: most vertices take one round
+                const uint64_t want = S ? 2 * ((qEdges + S - 1) / S) : 1;
+                const unsigned G = want <= 4 ? 4u : want <= 8 ? 8u : want <= 16 ? 16u : 32u;
+                tdGroups(a, S, G, qc, level, cur, a.bm[(level + 1) % 3], acc, fedges >= 65536);
             }
             const uint32_t nt = warpMode ? 0u : (S + NT - 1) / NT;
             const uint64_t HC = (uint64_t)NT * 2;
