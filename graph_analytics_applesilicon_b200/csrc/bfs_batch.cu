@@ -350,7 +350,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                 float f[kSelFeatures];
                 selectorFeatures((double)size, (double)fedges, (double)(a.m > fullEdges ? a.m - fullEdges : 0),
                                  (double)(a.n - fullCount), (double)a.n, (double)a.m, (double)level, f);
-                const int s = selectorChoose(sm.sel, f, tid, bottomUp, a.selMargin);
+                // trust region: bottom-up only within 4x of the rule's threshold
+                const bool mayGoBU = (double)scout * 4.0 > (double)toCheck / a.alpha;
+                const int s = selectorChoose(sm.sel, f, tid, bottomUp, a.selMargin, mayGoBU);
                 if (tid == 0) sm.strat = s;
             }
             __syncthreads();

@@ -475,7 +475,12 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
             float f[kSelFeatures];
             selectorFeatures((double)size, (double)fedges, (double)unexplored, (double)(a.n - reached), (double)a.n,
                              (double)a.m, (double)level, f);
-            int s = selectorChoose(sm.sel, f, tid, bottomUp, a.selMargin);
+            // trust region: a top-down level may go bottom-up only when its
+            // edges are within 4x of the rule's threshold (toCheck / alpha);
+            // far below it bottom-up would scan every unvisited vertex for a
+            // small frontier
+            const bool mayGoBU = (double)scout * 4.0 > (double)toCheck / a.alpha;
+            int s = selectorChoose(sm.sel, f, tid, bottomUp, a.selMargin, mayGoBU);
             if (tid == 0) sm.strat = s;
         }
         if (tid == 0) sm.acc[0] = sm.acc[1] = sm.acc[2] = 0;

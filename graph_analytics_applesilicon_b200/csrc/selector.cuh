@@ -66,13 +66,14 @@ __device__ __forceinline__ void selectorStage(float* S, const float* P, unsigned
 
 // One warp evaluates the MLP (lane j owns hidden unit j) on the features of
 // a level and returns the strategy to run, or -1 if an output is not finite.
-// ruleBU is the alpha/beta rule's direction; with margin 0 the result is the
-// strategy of smallest predicted time.
+// ruleBU is the alpha/beta rule's direction; with margin 0 (and mayGoBU) the
+// result is the strategy of smallest predicted time.  mayGoBU = false keeps a
+// top-down level top-down (the caller's trust region around the rule).
 // S is the shared-memory copy written by selectorStage.  Every lane returns
 // the same value; the result depends only on the parameters and f, so every
 // block of a grid that calls it on the same counters agrees.
 __device__ __forceinline__ int selectorChoose(const float* S, const float* f, unsigned lane, bool ruleBU,
-                                              float margin) {
+                                              float margin, bool mayGoBU = true) {
     const float* w1 = S;  // [k][j]
     const float* b1 = w1 + kSelHidden * kSelFeatures;
     const float* w2 = b1 + kSelHidden;  // [k][j]
@@ -110,7 +111,7 @@ __device__ __forceinline__ int selectorChoose(const float* S, const float* f, un
     }
     const float tBU = __shfl_sync(kFull, out, GB_STRAT_BU);
     if (ruleBU) return key + margin < tBU ? idx : GB_STRAT_BU;
-    return tBU + margin < key ? GB_STRAT_BU : idx;
+    return mayGoBU && tBU + margin < key ? GB_STRAT_BU : idx;
 }
 #endif
 
