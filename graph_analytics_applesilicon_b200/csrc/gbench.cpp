@@ -9,7 +9,7 @@
 //
 // GPU variants call the B200 library through include/graph_b200.hpp.  New:
 // gpu_do_persistent (and hybrid, which maps to it), --selector rule|learned,
-// --batch 64 (sources in batches of up to 64 per launch), --block, --hub-min,
+// --batch 64 (sources in batches of up to 64 per launch), --block, --hub-min, --grid-blocks, --sel-margin,
 // gpu_pull_f64, gpu_pull_blocked, and the benchmark graphs synth:rmat22, synth:road1400,
 // synth:web875k, synth:chunglu3m.  cpu_serial / cpu_omp / cpu_do are this
 // program's own CPU implementations of the reference's CPU variants
@@ -380,6 +380,7 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
     o.block = (uint32_t)args.getInt("block", 512);
     o.hub_min = (uint32_t)args.getInt("hub-min", 4096);
     o.grid_blocks = (uint32_t)args.getInt("grid-blocks", 0);
+    o.sel_margin = (float)args.getDouble("sel-margin", o.sel_margin);
     const std::string sel = args.get("selector", "rule");
     if (sel != "rule" && sel != "learned") throw std::runtime_error("--selector must be rule or learned");
     o.selector = sel == "learned" ? GB_SELECT_LEARNED : GB_SELECT_RULE;
