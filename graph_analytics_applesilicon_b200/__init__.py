@@ -116,6 +116,10 @@ def lib():
             "gb_csr_transpose": (C.c_int, [P, P]),
             "gb_csr_symmetrize": (C.c_int, [P, P]),
             "gb_csr_permute": (C.c_int, [P, _u32p, P]),
+            "gb_csr_from_edges_gpu": (C.c_int, [C.c_uint64, _u32p, _u32p, C.c_uint64, C.c_int, P]),
+            "gb_csr_transpose_gpu": (C.c_int, [P, P]),
+            "gb_csr_symmetrize_gpu": (C.c_int, [P, P]),
+            "gb_csr_permute_gpu": (C.c_int, [P, _u32p, P]),
             "gb_random_perm": (C.c_int, [C.c_uint64, C.c_uint64, _u32p]),
             "gb_gen_path": (C.c_int, [C.c_uint32, P]),
             "gb_gen_star": (C.c_int, [C.c_uint32, P]),
@@ -297,6 +301,28 @@ def symmetrize(g: Graph) -> Graph:
 
 def permute(g: Graph, perm) -> Graph:
     return _make(lib().gb_csr_permute, C.byref(g._c()), np.ascontiguousarray(perm, np.uint32))
+
+
+# The same operations on the GPU (gb_csr_*_gpu): identical results.
+def from_edges_gpu(n, eu, ev, directed=False) -> Graph:
+    eu = np.ascontiguousarray(eu, np.uint32)
+    ev = np.ascontiguousarray(ev, np.uint32)
+    k = eu.size
+    if k == 0:
+        eu = ev = np.zeros(1, np.uint32)
+    return _make(lib().gb_csr_from_edges_gpu, n, eu, ev, k, int(directed))
+
+
+def transpose_gpu(g: Graph) -> Graph:
+    return _make(lib().gb_csr_transpose_gpu, C.byref(g._c()))
+
+
+def symmetrize_gpu(g: Graph) -> Graph:
+    return _make(lib().gb_csr_symmetrize_gpu, C.byref(g._c()))
+
+
+def permute_gpu(g: Graph, perm) -> Graph:
+    return _make(lib().gb_csr_permute_gpu, C.byref(g._c()), np.ascontiguousarray(perm, np.uint32))
 
 
 def random_perm(n: int, seed: int = 1) -> np.ndarray:

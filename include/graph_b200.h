@@ -66,6 +66,19 @@ int gb_csr_from_edges(uint64_t n, const uint32_t* eu, const uint32_t* ev, uint64
 int gb_csr_transpose(const gb_csr* g, gb_csr* out);
 int gb_csr_symmetrize(const gb_csr* g, gb_csr* out);
 int gb_csr_permute(const gb_csr* g, const uint32_t* perm, gb_csr* out);
+/* The same four operations on the GPU (host arrays in and out, results
+ * identical to the functions above): one 64-bit (row, column) key per output
+ * entry, a radix sort, then the duplicate / self-loop rule of each operation.
+ * fromEdgeList (src/graph/csr.cpp:146-163), transpose, symmetrize and permute
+ * (src/graph/transform.cpp:9-76).  gb_csr_symmetrize_gpu needs a
+ * duplicate-free directed input (flag bit 2), as every generator and
+ * fromEdgeList produce; undirected inputs come back unchanged.  Inputs are
+ * checked on the host (ids below n, row_ptr from 0 to m). */
+int gb_csr_from_edges_gpu(uint64_t n, const uint32_t* eu, const uint32_t* ev, uint64_t ne, int directed,
+                          gb_csr* out);
+int gb_csr_transpose_gpu(const gb_csr* g, gb_csr* out);
+int gb_csr_symmetrize_gpu(const gb_csr* g, gb_csr* out);
+int gb_csr_permute_gpu(const gb_csr* g, const uint32_t* perm, gb_csr* out);
 /* reorder::compute(..., "random", seed) (src/graph/reorder.cpp:20-25). */
 int gb_random_perm(uint64_t n, uint64_t seed, uint32_t* perm);
 
