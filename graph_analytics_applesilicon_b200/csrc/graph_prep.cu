@@ -142,6 +142,37 @@ __global__ void edgeKeysKernel(const uint32_t* eu, const uint32_t* ev, uint64_t 
     }
 }
 
+// Input checks on the device (every id that reaches the key kernels must be
+// below n): bad |= 1 row_ptr decreases, 2 column >= n, 4 edge endpoint >= n,
+// 8 perm value >= n or repeated (seen: ceil(n/32) zeroed words).
+__global__ void checkCsrKernel(const uint32_t* rp, const uint32_t* ci, uint64_t n, uint64_t m, unsigned* bad) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    unsigned f = 0;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        if (rp[v] > rp[v + 1]) f |= 1u;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+        if (ci[i] >= n) f |= 2u;
+    if (f) atomicOr(bad, f);
+}
+
+__global__ void checkEdgesKernel(const uint32_t* eu, const uint32_t* ev, uint64_t ne, uint64_t n, unsigned* bad) {
+    unsigned f = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += (uint64_t)gridDim.x * blockDim.x)
+        if (eu[i] >= n || ev[i] >= n) f |= 4u;
+    if (f) atomicOr(bad, f);
+}
+
+__global__ void checkPermKernel(const uint32_t* perm, uint64_t n, uint32_t* seen, unsigned* bad) {
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = perm[v];
+        if (p >= n) {
+            atomicOr(bad, 8u);
+            continue;
+        }
+        if (atomicOr(&seen[p >> 5], 1u << (p & 31)) & (1u << (p & 31))) atomicOr(bad, 8u);
+    }
+}
+
 uint32_t gridOf(uint64_t work, uint32_t threads) {
     const uint64_t g = (work + threads - 1) / threads;
     return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(g, (uint64_t)deviceSmCount() * 16));
@@ -217,14 +248,15 @@ void keysToCsr(DevBuf<unsigned long long>& keys, uint64_t N, uint64_t n, int b, 
     out->col_idx = hci;
 }
 
-// Every id that reaches the device must be < n (the kernels index row
-// counters with them): row_ptr monotone from 0 to m, columns below n.
-void checkCsr(const gb_csr* g) {
-    GB_REQUIRE(g->row_ptr && (g->m == 0 || g->col_idx), "null CSR arrays");
-    GB_REQUIRE(g->row_ptr[0] == 0 && g->row_ptr[g->n] == g->m, "graph prep: row_ptr must run from 0 to m");
-    for (uint64_t v = 0; v < g->n; ++v)
-        GB_REQUIRE(g->row_ptr[v] <= g->row_ptr[v + 1], "graph prep: row_ptr must not decrease");
-    for (uint64_t i = 0; i < g->m; ++i) GB_REQUIRE(g->col_idx[i] < g->n, "graph prep: column id >= n");
+// Reads the device check word; throws if any check failed.
+void requireChecks(DevBuf<unsigned>& bad, cudaStream_t st) {
+    unsigned h = 0;
+    GB_CUDA(cudaMemcpyAsync(&h, bad.get(), 4, cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaStreamSynchronize(st));
+    if (h & 1u) throw Error(GB_ERR_ARG, "graph prep: row_ptr must not decrease");
+    if (h & 2u) throw Error(GB_ERR_ARG, "graph prep: column id >= n");
+    if (h & 4u) throw Error(GB_ERR_ARG, "gb_csr_from_edges_gpu: edge endpoint >= n");
+    if (h & 8u) throw Error(GB_ERR_ARG, "gb_csr_permute_gpu: perm is not a permutation of [0, n)");
 }
 
 // Uploads a host CSR.
@@ -243,15 +275,26 @@ void csrOp(const gb_csr* g, int mode, const uint32_t* permHost, bool unique, boo
     GB_REQUIRE(g && out, "null argument");
     GB_REQUIRE(g->n >= 1 && g->n < 0xFFFFFFFFull, "graph prep: n must be in [1, 2^32 - 1)");
     GB_REQUIRE(g->m < (1ull << 32), "graph prep: m must fit in uint32");
-    checkCsr(g);
+    GB_REQUIRE(g->row_ptr && (g->m == 0 || g->col_idx), "null CSR arrays");
+    GB_REQUIRE(g->row_ptr[0] == 0 && g->row_ptr[g->n] == g->m, "graph prep: row_ptr must run from 0 to m");
     Stream st;
     ScanScratch sc;
-    DevBuf<uint32_t> rp, ci, perm;
+    DevBuf<uint32_t> rp, ci, perm, seen;
+    DevBuf<unsigned> bad;
+    bad.ensure(1);
+    GB_CUDA(cudaMemsetAsync(bad.get(), 0, 4, st.s));
     uploadCsr(g, rp, ci, st.s);
+    checkCsrKernel<<<gridOf(std::max(g->n, g->m), 256), 256, 0, st.s>>>(rp.get(), ci.get(), g->n, g->m, bad.get());
+    GB_LAUNCH_CHECK();
     if (mode == 2) {
         perm.ensure(g->n);
+        seen.ensure((g->n + 31) / 32);
         GB_CUDA(cudaMemcpyAsync(perm.get(), permHost, g->n * 4, cudaMemcpyHostToDevice, st.s));
+        GB_CUDA(cudaMemsetAsync(seen.get(), 0, (g->n + 31) / 32 * 4, st.s));
+        checkPermKernel<<<gridOf(g->n, 256), 256, 0, st.s>>>(perm.get(), g->n, seen.get(), bad.get());
+        GB_LAUNCH_CHECK();
     }
+    requireChecks(bad, st.s);
     const int b = bitsFor(g->n);
     const uint64_t N = mode == 3 ? 2 * g->m : g->m;
     DevBuf<unsigned long long> keys, tmp;
@@ -277,17 +320,21 @@ int gb_csr_from_edges_gpu(uint64_t n, const uint32_t* eu, const uint32_t* ev, ui
     return guard([&] {
         GB_REQUIRE(out && (ne == 0 || (eu && ev)), "null argument");
         GB_REQUIRE(n >= 1 && n < 0xFFFFFFFFull, "graph prep: n must be in [1, 2^32 - 1)");
-        for (uint64_t i = 0; i < ne; ++i)
-            GB_REQUIRE(eu[i] < n && ev[i] < n, "gb_csr_from_edges_gpu: edge endpoint >= n");
         Stream st;
         ScanScratch sc;
         DevBuf<uint32_t> du, dv;
+        DevBuf<unsigned> bad;
+        bad.ensure(1);
         du.ensure(ne + 1);
         dv.ensure(ne + 1);
+        GB_CUDA(cudaMemsetAsync(bad.get(), 0, 4, st.s));
         if (ne) {
             GB_CUDA(cudaMemcpyAsync(du.get(), eu, ne * 4, cudaMemcpyHostToDevice, st.s));
             GB_CUDA(cudaMemcpyAsync(dv.get(), ev, ne * 4, cudaMemcpyHostToDevice, st.s));
+            checkEdgesKernel<<<gridOf(ne, 256), 256, 0, st.s>>>(du.get(), dv.get(), ne, n, bad.get());
+            GB_LAUNCH_CHECK();
         }
+        requireChecks(bad, st.s);
         const int b = bitsFor(n);
         const uint64_t N = directed ? ne : 2 * ne;
         DevBuf<unsigned long long> keys, tmp;
@@ -335,12 +382,7 @@ int gb_csr_symmetrize_gpu(const gb_csr* g, gb_csr* out) {
 int gb_csr_permute_gpu(const gb_csr* g, const uint32_t* perm, gb_csr* out) {
     return guard([&] {
         GB_REQUIRE(g && perm, "null argument");
-        std::vector<uint8_t> seen(g->n, 0);  // perm must be a permutation of [0, n)
-        for (uint64_t v = 0; v < g->n; ++v) {
-            GB_REQUIRE(perm[v] < g->n && !seen[perm[v]], "gb_csr_permute_gpu: perm is not a permutation of [0, n)");
-            seen[perm[v]] = 1;
-        }
-        csrOp(g, 2, perm, false, false, g->flags, out);
+        csrOp(g, 2, perm, false, false, g->flags, out);  // perm is checked on the device
     });
 }
 

@@ -73,7 +73,8 @@ int gb_csr_permute(const gb_csr* g, const uint32_t* perm, gb_csr* out);
  * (src/graph/transform.cpp:9-76).  gb_csr_symmetrize_gpu needs a
  * duplicate-free directed input (flag bit 2), as every generator and
  * fromEdgeList produce; undirected inputs come back unchanged.  Inputs are
- * checked on the host (ids below n, row_ptr from 0 to m). */
+ * checked on the device before use (ids below n, row_ptr from 0 to m, perm a
+ * permutation). */
 int gb_csr_from_edges_gpu(uint64_t n, const uint32_t* eu, const uint32_t* ev, uint64_t ne, int directed,
                           gb_csr* out);
 int gb_csr_transpose_gpu(const gb_csr* g, gb_csr* out);

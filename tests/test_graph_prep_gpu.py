@@ -65,3 +65,9 @@ def test_errors(gb):
         gb.permute_gpu(g, np.zeros(10, np.uint32))        # not a permutation
     with pytest.raises(gb.GraphError):
         gb.from_edges_gpu(5, [1, 7], [2, 3])              # endpoint >= n
+    bad = gb.gen.path(10)
+    bad.col_idx = bad.col_idx.copy()
+    bad.col_idx[3] = 99                                   # column >= n
+    with pytest.raises(gb.GraphError):
+        gb.transpose_gpu(bad)
+    assert same(gb.transpose_gpu(g), gb.transpose(g))     # the context is still usable
