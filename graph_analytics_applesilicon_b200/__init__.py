@@ -120,6 +120,7 @@ def lib():
             "gb_csr_transpose_gpu": (C.c_int, [P, P]),
             "gb_csr_symmetrize_gpu": (C.c_int, [P, P]),
             "gb_csr_permute_gpu": (C.c_int, [P, _u32p, P]),
+            "gb_pick_sources_gpu": (C.c_int, [P, C.c_int, C.c_uint64, C.c_int, _u32p, C.POINTER(C.c_int)]),
             "gb_random_perm": (C.c_int, [C.c_uint64, C.c_uint64, _u32p]),
             "gb_gen_path": (C.c_int, [C.c_uint32, P]),
             "gb_gen_star": (C.c_int, [C.c_uint32, P]),
@@ -349,6 +350,14 @@ def pick_sources(g: Graph, count=64, seed=1, any_component=False) -> np.ndarray:
     out = np.zeros(max(count, 1), np.uint32)
     k = C.c_int(0)
     check(lib().gb_pick_sources(C.byref(g._c()), count, seed, int(any_component), out, C.byref(k)))
+    return out[: k.value]
+
+
+def pick_sources_gpu(g: Graph, count=64, seed=1, any_component=False) -> np.ndarray:
+    """pick_sources with the largest component found on the GPU (same result)."""
+    out = np.zeros(max(count, 1), np.uint32)
+    k = C.c_int(0)
+    check(lib().gb_pick_sources_gpu(C.byref(g._c()), count, seed, int(any_component), out, C.byref(k)))
     return out[: k.value]
 
 

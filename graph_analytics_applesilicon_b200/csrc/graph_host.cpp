@@ -548,15 +548,22 @@ std::vector<uint32_t> pickSources(const HostCsr& g, int count, uint64_t seed, bo
         }
         for (uint64_t v = 0; v < n; ++v) ok[v] = comp[v] == best;
     }
+    return drawSources(n, g.row_ptr.data(), ok, count, seed);
+}
+
+// The drawing half of pickSources: distinct vertices v = below(n) in the
+// seeded stream, kept when ok[v] and degree(v) > 0.
+std::vector<uint32_t> drawSources(uint64_t n, const uint32_t* row_ptr, const std::vector<uint8_t>& ok, int count,
+                                  uint64_t seed) {
     uint64_t candidates = 0;
-    for (uint64_t v = 0; v < n; ++v) candidates += ok[v] && g.degree(v) > 0;
+    for (uint64_t v = 0; v < n; ++v) candidates += ok[v] && row_ptr[v + 1] > row_ptr[v];
     count = (int)std::min<uint64_t>((uint64_t)std::max(count, 0), candidates);
     std::vector<uint32_t> out;
     std::vector<uint8_t> used(n, 0);
     uint64_t k = 0;
     while ((int)out.size() < count) {
         uint32_t v = (uint32_t)belowAt(seed, ++k, n);
-        if (ok[v] && g.degree(v) > 0 && !used[v]) {
+        if (ok[v] && row_ptr[v + 1] > row_ptr[v] && !used[v]) {
             used[v] = 1;
             out.push_back(v);
         }

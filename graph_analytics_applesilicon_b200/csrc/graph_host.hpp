@@ -54,5 +54,7 @@ void csrSave(const HostCsr& g, const std::string& path);
 HostCsr csrLoad(const std::string& path);
 
 std::vector<uint32_t> pickSources(const HostCsr& g, int count, uint64_t seed, bool anyComponent);
+std::vector<uint32_t> drawSources(uint64_t n, const uint32_t* row_ptr, const std::vector<uint8_t>& ok, int count,
+                                  uint64_t seed);
 
 }  // namespace gb

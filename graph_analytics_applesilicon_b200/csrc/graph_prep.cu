@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "capi_util.hpp"
+#include "graph_host.hpp"
 #include "prims.cuh"
 
 namespace gb {
@@ -111,6 +112,11 @@ __global__ void rsEmitKernel(const unsigned long long* keys, uint64_t n, int b, 
     }
 }
 
+__global__ void initIotaKernel(uint32_t* p, uint64_t n) {
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+        p[v] = (uint32_t)v;
+}
+
 // Keys of a CSR's entries: (map(row) or col-as-row) per mode.
 //   mode 0: (row, col)             mode 1: (col, row)  (transpose)
 //   mode 2: (perm[row], perm[col])  mode 3: (row, col) and (col, row) (symmetrize)
@@ -171,6 +177,66 @@ __global__ void checkPermKernel(const uint32_t* perm, uint64_t n, uint32_t* seen
         }
         if (atomicOr(&seen[p >> 5], 1u << (p & 31)) & (1u << (p & 31))) atomicOr(bad, 8u);
     }
+}
+
+// Connected components (symmetric graph) by hooking and pointer jumping:
+// every edge hooks the larger of its endpoints' roots under the smaller
+// (atomicMin), then every vertex jumps to its root; repeated until no hook
+// changes anything.  A root only ever moves to a smaller id, so each
+// component ends rooted at its smallest vertex: the reference's component
+// order (components numbered by their first, i.e. smallest, vertex).
+__device__ __forceinline__ uint32_t ccRoot(const uint32_t* parent, uint32_t v) {
+    uint32_t p = parent[v];
+    while (p != v) {
+        v = p;
+        p = parent[v];
+    }
+    return v;
+}
+
+__global__ void ccHookKernel(const uint32_t* rp, const uint32_t* ci, uint64_t n, uint32_t* parent, unsigned* changed) {
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    bool any = false;
+    for (uint64_t u = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += nw) {
+        for (uint32_t i = rp[u] + lane; i < rp[u + 1]; i += 32) {
+            const uint32_t v = ci[i];
+            if (v <= u) continue;  // each undirected edge once
+            const uint32_t ru = ccRoot(parent, (uint32_t)u), rv = ccRoot(parent, v);
+            if (ru == rv) continue;
+            const uint32_t hi = ru > rv ? ru : rv, lo = ru > rv ? rv : ru;
+            if (atomicMin(&parent[hi], lo) > lo) any = true;
+        }
+    }
+    if (__any_sync(0xFFFFFFFFu, any) && lane == 0) atomicOr(changed, 1u);
+}
+
+__global__ void ccJumpKernel(uint64_t n, uint32_t* parent) {
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+        parent[v] = ccRoot(parent, (uint32_t)v);
+}
+
+// size per root, then the best (largest; the smallest root among equals)
+// packed as (size << 32) | (~root) into one atomicMax.
+__global__ void ccSizeKernel(uint64_t n, const uint32_t* parent, uint32_t* size) {
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&size[parent[v]], 1u);
+}
+
+__global__ void ccBestKernel(uint64_t n, const uint32_t* size, unsigned long long* best) {
+    unsigned long long b = 0;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+        if (size[v]) {
+            const unsigned long long key = ((unsigned long long)size[v] << 32) | (0xFFFFFFFFu - (uint32_t)v);
+            b = key > b ? key : b;
+        }
+    if (b) atomicMax(best, b);
+}
+
+__global__ void ccMaskKernel(uint64_t n, const uint32_t* parent, const unsigned long long* best, uint8_t* ok) {
+    const uint32_t root = 0xFFFFFFFFu - (uint32_t)(*best & 0xFFFFFFFFull);
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+        ok[v] = parent[v] == root ? 1 : 0;
 }
 
 uint32_t gridOf(uint64_t work, uint32_t threads) {
@@ -383,6 +449,67 @@ int gb_csr_permute_gpu(const gb_csr* g, const uint32_t* perm, gb_csr* out) {
     return guard([&] {
         GB_REQUIRE(g && perm, "null argument");
         csrOp(g, 2, perm, false, false, g->flags, out);  // perm is checked on the device
+    });
+}
+
+int gb_pick_sources_gpu(const gb_csr* g, int count, uint64_t seed, int any_component, uint32_t* out, int* k) {
+    return guard([&] {
+        GB_REQUIRE(g && g->row_ptr && out, "null argument");
+        GB_REQUIRE(g->n >= 1 && g->n < 0xFFFFFFFFull, "graph prep: n must be in [1, 2^32 - 1)");
+        GB_REQUIRE(g->row_ptr[0] == 0 && g->row_ptr[g->n] == g->m, "graph prep: row_ptr must run from 0 to m");
+        const uint64_t n = g->n;
+        std::vector<uint8_t> ok(n, 1);
+        if (!any_component) {
+            GB_REQUIRE(!(g->flags & kFlagDirected),
+                       "gb_pick_sources_gpu: components need a symmetric graph (gb_pick_sources follows "
+                       "out-edges of directed ones)");
+            Stream st;
+            DevBuf<uint32_t> rp, ci, parent, size;
+            DevBuf<unsigned> bad, changed;
+            DevBuf<unsigned long long> best;
+            DevBuf<uint8_t> dok;
+            bad.ensure(1);
+            changed.ensure(1);
+            best.ensure(1);
+            GB_CUDA(cudaMemsetAsync(bad.get(), 0, 4, st.s));
+            uploadCsr(g, rp, ci, st.s);
+            checkCsrKernel<<<gridOf(std::max(n, g->m), 256), 256, 0, st.s>>>(rp.get(), ci.get(), n, g->m, bad.get());
+            GB_LAUNCH_CHECK();
+            requireChecks(bad, st.s);
+            parent.ensure(n);
+            size.ensure(n);
+            dok.ensure(n);
+            initIotaKernel<<<gridOf(n, 256), 256, 0, st.s>>>(parent.get(), n);
+            GB_LAUNCH_CHECK();
+            // hook + jump rounds; each round at least halves the number of
+            // roots that still have a smaller neighbouring root, so 64 rounds
+            // cover any n < 2^32 many times over
+            bool done = false;
+            for (int round = 0; round < 64 && !done; ++round) {
+                GB_CUDA(cudaMemsetAsync(changed.get(), 0, 4, st.s));
+                ccHookKernel<<<gridOf(n * 32, 256), 256, 0, st.s>>>(rp.get(), ci.get(), n, parent.get(),
+                                                                      changed.get());
+                GB_LAUNCH_CHECK();
+                ccJumpKernel<<<gridOf(n, 256), 256, 0, st.s>>>(n, parent.get());
+                GB_LAUNCH_CHECK();
+                unsigned h = 0;
+                GB_CUDA(cudaMemcpyAsync(&h, changed.get(), 4, cudaMemcpyDeviceToHost, st.s));
+                GB_CUDA(cudaStreamSynchronize(st.s));
+                done = h == 0;
+            }
+            if (!done) throw Error(GB_ERR_STATE, "gb_pick_sources_gpu: components did not settle in 64 rounds");
+            GB_CUDA(cudaMemsetAsync(size.get(), 0, n * 4, st.s));
+            GB_CUDA(cudaMemsetAsync(best.get(), 0, 8, st.s));
+            ccSizeKernel<<<gridOf(n, 256), 256, 0, st.s>>>(n, parent.get(), size.get());
+            ccBestKernel<<<gridOf(n, 256), 256, 0, st.s>>>(n, size.get(), best.get());
+            ccMaskKernel<<<gridOf(n, 256), 256, 0, st.s>>>(n, parent.get(), best.get(), dok.get());
+            GB_LAUNCH_CHECK();
+            GB_CUDA(cudaMemcpyAsync(ok.data(), dok.get(), n, cudaMemcpyDeviceToHost, st.s));
+            GB_CUDA(cudaStreamSynchronize(st.s));
+        }
+        auto s = drawSources(n, g->row_ptr, ok, count, seed);
+        if (!s.empty()) std::memcpy(out, s.data(), s.size() * 4);
+        if (k) *k = (int)s.size();
     });
 }
 

@@ -80,6 +80,12 @@ int gb_csr_from_edges_gpu(uint64_t n, const uint32_t* eu, const uint32_t* ev, ui
 int gb_csr_transpose_gpu(const gb_csr* g, gb_csr* out);
 int gb_csr_symmetrize_gpu(const gb_csr* g, gb_csr* out);
 int gb_csr_permute_gpu(const gb_csr* g, const uint32_t* perm, gb_csr* out);
+/* gb_pick_sources with the largest connected component found on the GPU
+ * (largestComponent, src/bench/main.cpp:130-149: hooking + pointer jumping,
+ * components rooted at their smallest vertex, the first of the largest kept);
+ * same sources as gb_pick_sources.  Symmetric graphs only. */
+int gb_pick_sources_gpu(const gb_csr* g, int count, uint64_t seed, int any_component, uint32_t* out,
+                        int* k);
 /* reorder::compute(..., "random", seed) (src/graph/reorder.cpp:20-25). */
 int gb_random_perm(uint64_t n, uint64_t seed, uint32_t* perm);
 

@@ -59,6 +59,20 @@ def test_benchmark_graph(gb, golden):
     assert same(gb.transpose_gpu(g), g)
 
 
+def test_pick_sources_gpu_matches_host(gb):
+    """Sources from the largest component found on the GPU equal gb_pick_sources'
+    (gbench's largestComponent + pickSources) on graphs with many components,
+    equal-sized components, isolated vertices and long paths."""
+    graphs = [g if not g.directed else gb.symmetrize(g) for _, g in gb.gen.suite()]
+    graphs += [gb.gen.road(300, 300, 0.04, 0.005, 3), gb.gen.road(400, 400, 0.3, 0.0, 4),
+               gb.from_edges(12, [0, 2, 4, 6], [1, 3, 5, 7]),          # equal components: the first wins
+               gb.gen.path(200000), gb.gen.rmat(18, 4, False, 9)]
+    for g in graphs:
+        for count, seed in ((64, 1), (8, 7)):
+            assert np.array_equal(gb.pick_sources_gpu(g, count, seed), gb.pick_sources(g, count, seed)), (g.n, g.m)
+        assert np.array_equal(gb.pick_sources_gpu(g, 16, 3, True), gb.pick_sources(g, 16, 3, True))
+
+
 def test_errors(gb):
     g = gb.gen.path(10)
     with pytest.raises(gb.GraphError):
@@ -71,3 +85,5 @@ def test_errors(gb):
     with pytest.raises(gb.GraphError):
         gb.transpose_gpu(bad)
     assert same(gb.transpose_gpu(g), gb.transpose(g))     # the context is still usable
+    with pytest.raises(gb.GraphError):
+        gb.pick_sources_gpu(gb.gen.rmat(10, 8, True, 1))   # directed: not supported
