@@ -111,12 +111,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_graph(G, scale=SCALE, nsrc=NSRC):
+def build_graph(G, scale=SCALE, nsrc=NSRC, gpu_prep=True):
+    """The benchmark graph and its sources.  gpu_prep permutes and picks sources
+    with the library's GPU preparation (identical results); the reference arm
+    passes False so that its set-up runs on the host only."""
     t = time.time()
     edges = EDGES_DRAWN if scale == SCALE else int(8.5 * (1 << scale))
     g = G.gen.rmat(scale, edges=edges, directed=False, seed=GEN_SEED)
-    g = G.permute(g, G.random_perm(g.n, PERM_SEED))
-    srcs = G.pick_sources(g, nsrc, 1)
+    perm = G.random_perm(g.n, PERM_SEED)
+    g = G.permute_gpu(g, perm) if gpu_prep else G.permute(g, perm)
+    srcs = G.pick_sources_gpu(g, nsrc, 1) if gpu_prep else G.pick_sources(g, nsrc, 1)
     log(f"graph n={g.n} m={g.m} built in {time.time() - t:.1f}s")
     return g, srcs
 
@@ -222,7 +226,7 @@ def reference_arm(args, world, rank):
     if rank != 0:
         return
     import graph_analytics_applesilicon_b200 as G
-    g, srcs = build_graph(G)
+    g, srcs = build_graph(G, gpu_prep=False)
     per_step = 20.0 / max(1, args.steps + args.warmup)
     for _ in range(args.warmup):
         cpu_baseline(g, srcs, per_step)
@@ -266,7 +270,7 @@ def bfs_config_workload(args, world, rank, local):
     road = args.workload == "road_bfs"
     g = G.gen.road(1400, 1400, 0.04, 0.005, 1400) if road else G.gen.chung_lu(3070000, 2.2, 76.0, 307)
     log(f"{args.workload}: n={g.n} m={g.m} built in {time.time() - t:.1f}s")
-    srcs64 = G.pick_sources(g, 64, 1)
+    srcs64 = G.pick_sources_gpu(g, 64, 1)
     bfs = G.GpuBfs(g)
     comp = {int(s): component_edges(g, bfs.run("gpu_do_persistent", int(s))) for s in srcs64}
     sel1, sel2 = G.default_selector_params("single"), G.default_selector_params("batch")
@@ -358,7 +362,7 @@ def pagerank_tol_workload(args, world, rank, local):
     import graph_analytics_applesilicon_b200 as G
     torch.cuda.set_device(local)
     g = G.gen.web(875000, 5.8, 2.1, 875)
-    gin = G.transpose(g)
+    gin = G.transpose_gpu(g)
     pr = G.GpuPageRank(g.n, g, gin, g.degrees())
     pr.prepareGS(2)
     o = G.PrOptions(tol=1e-6, iters=1000)

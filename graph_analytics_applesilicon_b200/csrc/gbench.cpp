@@ -11,7 +11,9 @@
 // gpu_do_persistent (and hybrid, which maps to it), --selector rule|learned,
 // --batch 64 (sources in batches of up to 64 per launch), --block, --hub-min, --grid-blocks, --sel-margin,
 // gpu_pull_f64, gpu_pull_blocked, and the benchmark graphs synth:rmat22, synth:road1400,
-// synth:web875k, synth:chunglu3m.  cpu_serial / cpu_omp / cpu_do are this
+// synth:web875k, synth:chunglu3m.  Graph preparation (symmetrize, transpose,
+// permute, source picking) runs on the GPU; --host-prep keeps it on the host.
+// cpu_serial / cpu_omp / cpu_do are this
 // program's own CPU implementations of the reference's CPU variants
 // (src/cpu/bfs_cpu.cpp, src/cpu/pagerank_cpu.cpp); --validate uses cpu_serial.
 #include <omp.h>
@@ -97,6 +99,25 @@ double msSince(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Graph preparation runs on the GPU (gb_csr_*_gpu, identical results) unless
+// --host-prep is given; symmetrize of a directed list with repeated entries
+// (no duplicate-free flag) keeps the host merge, which defines that case.
+bool gHostPrep = false;
+int prepSymmetrize(const gb_csr* g, gb_csr* out) {
+    const bool gpuOk = !(g->flags & 1u) || (g->flags & 4u);
+    return (!gHostPrep && gpuOk) ? gb_csr_symmetrize_gpu(g, out) : gb_csr_symmetrize(g, out);
+}
+int prepTranspose(const gb_csr* g, gb_csr* out) {
+    return gHostPrep ? gb_csr_transpose(g, out) : gb_csr_transpose_gpu(g, out);
+}
+int prepPermute(const gb_csr* g, const uint32_t* perm, gb_csr* out) {
+    return gHostPrep ? gb_csr_permute(g, perm, out) : gb_csr_permute_gpu(g, perm, out);
+}
+int prepPickSources(const gb_csr* g, int count, uint64_t seed, int any, uint32_t* out, int* k) {
+    return (gHostPrep || (g->flags & 1u)) ? gb_pick_sources(g, count, seed, any, out, k)
+                                          : gb_pick_sources_gpu(g, count, seed, any, out, k);
+}
+
 Graph loadGraph(const std::string& spec, std::string& name) {
     if (spec.rfind("synth:", 0) == 0) {
         name = spec.substr(6);
@@ -112,7 +133,7 @@ Graph loadGraph(const std::string& spec, std::string& name) {
             Graph g = make([](gb_csr* o) { return gb_gen_rmat(22, 35651584ull, 0, 22, o); });
             std::vector<uint32_t> p(g.n());
             gpu::check(gb_random_perm(g.n(), 1, p.data()));
-            return make([&](gb_csr* o) { return gb_csr_permute(&g.c, p.data(), o); });
+            return make([&](gb_csr* o) { return prepPermute(&g.c, p.data(), o); });
         }
         if (name == "road1400") return make([](gb_csr* o) { return gb_gen_road(1400, 1400, 0.04, 0.005, 1400, o); });
         if (name == "web875k") return make([](gb_csr* o) { return gb_gen_web(875000, 5.8, 2.1, 875, o); });
@@ -387,7 +408,7 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
     const int batch = (int)args.getInt("batch", 0);
 
     auto prep0 = std::chrono::steady_clock::now();
-    Graph g = make([&](gb_csr* out) { return gb_csr_symmetrize(&stored.c, out); });
+    Graph g = make([&](gb_csr* out) { return prepSymmetrize(&stored.c, out); });
     std::vector<uint32_t> perm;
     const std::string ordering = args.get("ordering", "original");
     if (ordering == "random") {
@@ -399,7 +420,7 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
     Graph refG;  // original labels: sources, reference, TEPS denominators
     if (!perm.empty()) {
         refG = std::move(g);
-        g = make([&](gb_csr* out) { return gb_csr_permute(&refG.c, perm.data(), out); });
+        g = make([&](gb_csr* out) { return prepPermute(&refG.c, perm.data(), out); });
     }
     const Graph& R = perm.empty() ? g : refG;
     auto toRun = [&](uint32_t s) { return perm.empty() ? s : perm[s]; };
@@ -420,7 +441,7 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
     else {
         sources.resize(std::max<long long>(1, args.getInt("sources", 64)));
         int k = 0;
-        gpu::check(gb_pick_sources(&R.c, (int)sources.size(), (uint64_t)args.getInt("seed", 1),
+        gpu::check(prepPickSources(&R.c, (int)sources.size(), (uint64_t)args.getInt("seed", 1),
                                    args.has("any-component"), sources.data(), &k));
         sources.resize(k);
     }
@@ -656,8 +677,8 @@ int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
     const bool gsCheck = variant == "gpu_pull_gs" || o.inplace;
 
     auto prep0 = std::chrono::steady_clock::now();
-    Graph in = stored.directed() ? make([&](gb_csr* out) { return gb_csr_transpose(&stored.c, out); })
-                                 : make([&](gb_csr* out) { return gb_csr_permute(&stored.c, [&] {
+    Graph in = stored.directed() ? make([&](gb_csr* out) { return prepTranspose(&stored.c, out); })
+                                 : make([&](gb_csr* out) { return prepPermute(&stored.c, [&] {
                                        static std::vector<uint32_t> id;
                                        id.resize(stored.n());
                                        std::iota(id.begin(), id.end(), 0u);
@@ -762,6 +783,7 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "usage: gbench --graph <file.bin | synth:NAME> --algo bfs|pr --variant V [options]\n");
         return 2;
     }
+    gHostPrep = args.has("host-prep");
     try {
         std::string dataset;
         Graph g = loadGraph(args.get("graph"), dataset);
