@@ -352,6 +352,99 @@ def bfs_config_workload(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def edge_text(u, v) -> bytes:
+    """1-based 'u<TAB>v' lines, formatted with vectorised digit arithmetic."""
+    u = np.asarray(u, np.int64) + 1
+    v = np.asarray(v, np.int64) + 1
+    n, W = u.size, 10
+    rows = np.empty((n, 2 * W + 2), np.uint8)
+    for col, x in ((0, u), (W + 1, v)):
+        d = np.full((n, W), 0xFF, np.uint8)  # 0xFF: no digit (dropped below)
+        y = x.copy()
+        for k in range(W - 1, -1, -1):
+            has = (y > 0) | (k == W - 1)
+            d[has, k] = (48 + y[has] % 10).astype(np.uint8)
+            y //= 10
+        rows[:, col:col + W] = d
+    rows[:, W] = 9
+    rows[:, 2 * W + 1] = 10
+    flat = rows.reshape(-1)
+    return flat[flat != 0xFF].tobytes()
+
+
+def snap_convert_workload(args, world, rank, local):
+    """SNAP edge-list text -> CSR (graph::convertSnap, src/graph/snap.cpp:85-149,
+    the gconvert path): the undirected edges of the R-MAT scale-22 benchmark
+    graph, each written once (u < v) as a 1-based 'u<TAB>v' line (34.6M lines,
+    ~0.55 GB of plain text, read from the page cache), converted as undirected
+    to a .bin.  value: M edge lines/s of gb_convert_snap_gpu (read, H2D,
+    parse, relabel, sort, D2H, .bin write -- so value is also the end-to-end
+    number); cpu_baseline: the reference's own convertSnap (oracle/_ref, its
+    OpenMP compaction on all host cores) on the same file."""
+    import tempfile
+    import torch
+    import graph_analytics_applesilicon_b200 as G
+    torch.cuda.set_device(local)
+    g, _ = build_graph(G, nsrc=1)
+    rows = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(g.row_ptr.astype(np.int64)))
+    keep = rows < g.col_idx
+    u, v = rows[keep], g.col_idx[keep].astype(np.int64)
+    del rows, keep
+    tmp = tempfile.mkdtemp(prefix="snapbench_")
+    txt, out = os.path.join(tmp, "rmat22.txt"), os.path.join(tmp, "rmat22.bin")
+    t = time.time()
+    with open(txt, "wb") as f:
+        f.write(b"# R-MAT scale 22 benchmark graph, undirected edges once\n")
+        for i in range(0, u.size, 1 << 22):
+            f.write(edge_text(u[i:i + (1 << 22)], v[i:i + (1 << 22)]))
+    text_bytes, lines = os.path.getsize(txt), int(u.size)
+    log(f"snap text: {lines} lines, {text_bytes / 1e9:.2f} GB written in {time.time() - t:.1f}s")
+    st = None
+    for _ in range(args.warmup):
+        st = G.convert_snap_gpu(txt, out, False)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        st = G.convert_snap_gpu(txt, out, False)
+        ts.append(time.perf_counter() - t0)
+    conv = G.load(out)
+    # g is symmetric, so the conversion gives back g without its isolated
+    # vertices, the rest in the same order (relabelling by increasing raw id)
+    deg = np.diff(g.row_ptr.astype(np.int64))
+    ok = conv.n == int((deg > 0).sum()) and conv.m == g.m and st["lines"] == lines
+    if ok:
+        new = np.cumsum(deg > 0) - 1
+        ok = (bool(np.array_equal(conv.col_idx, new[g.col_idx].astype(np.uint32)))
+              and bool(np.array_equal(np.diff(conv.row_ptr.astype(np.int64)), deg[deg > 0])))
+    sec = max_over_ranks([statistics.median(ts)], world)[0]
+    value = world * lines / sec / 1e6
+    cpu = None
+    if rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_py as O
+        if O.ref_available():
+            t0 = time.perf_counter()
+            O.ref_convert_snap(txt, os.path.join(tmp, "ref.bin"), False)
+            rs = time.perf_counter() - t0
+            cpu = {"value": lines / rs / 1e6, "unit": "M lines/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"graph::convertSnap on the same {text_bytes / 1e9:.2f} GB file, one run, {rs:.1f}s"}
+            os.unlink(os.path.join(tmp, "ref.bin"))
+    for f in (txt, out):
+        os.unlink(f)
+    os.rmdir(tmp)
+    if rank != 0:
+        return
+    line = {"metric": "SNAP text -> CSR .bin conversion (gconvert)", "value": value, "unit": "M lines/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 text / u32 ids",
+            "data": "synthetic", "config": {"workload": "snap_rmat22_text", "lines": lines, "text_bytes": text_bytes,
+                                            "n": conv.n, "m": conv.m, "directed": False},
+            "e2e": {"value": value, "unit": "M lines/s", "h2d_bytes_per_step": text_bytes,
+                    "d2h_bytes_per_step": 4 * (conv.n + 1 + conv.m)},
+            "roofline": None, "cpu_baseline": cpu, "validated": ok, "stats": st}
+    print(json.dumps(line), flush=True)
+
+
 def pagerank_tol_workload(args, world, rank, local):
     """Web-shaped directed graph (875,000 vertices, geometric out-degree mean
     5.8 -> ~15% dangling, Zipf s=2.1 in-degree, seed 875): PageRank to tol 1e-6,
@@ -496,8 +589,9 @@ def main():
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (smaller: profiling cases)")
     ap.add_argument("--sources", type=int, default=NSRC)
     ap.add_argument("--workload", default=WORKLOAD,
-                    choices=[WORKLOAD, "chunglu_pr20", "road_bfs", "chunglu_bfs64", "web_pr_tol"],
-                    help="rmat22_bfs64 (default, the headline); chunglu_pr20, road_bfs, chunglu_bfs64, web_pr_tol")
+                    choices=[WORKLOAD, "chunglu_pr20", "road_bfs", "chunglu_bfs64", "web_pr_tol", "snap_convert"],
+                    help="rmat22_bfs64 (default, the headline); chunglu_pr20, road_bfs, chunglu_bfs64, web_pr_tol, "
+                         "snap_convert")
     ap.add_argument("--n", type=int, default=3070000, help="chunglu_pr20: vertices")
     args = ap.parse_args()
     world, rank, local = init_dist(args)
@@ -513,6 +607,9 @@ def main():
         return
     if args.workload == "web_pr_tol":
         pagerank_tol_workload(args, world, rank, local)
+        return
+    if args.workload == "snap_convert":
+        snap_convert_workload(args, world, rank, local)
         return
 
     import torch

@@ -44,6 +44,14 @@ class _Csr(C.Structure):
                 ("row_ptr", C.POINTER(C.c_uint32)), ("col_idx", C.POINTER(C.c_uint32))]
 
 
+class _ConvertStats(C.Structure):
+    _fields_ = [("lines", C.c_uint64), ("raw_max_id", C.c_uint64), ("n", C.c_uint64),
+                ("m_before", C.c_uint64), ("m", C.c_uint64), ("seconds", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class BfsOptions(C.Structure):
     """gb_bfs_options: GpuBfsOptions (src/metal/bfs_gpu.hpp:23-33) + new fields."""
     _fields_ = [("tg", C.c_uint32), ("small_max", C.c_uint32), ("large_min", C.c_uint32),
@@ -121,6 +129,8 @@ def lib():
             "gb_csr_symmetrize_gpu": (C.c_int, [P, P]),
             "gb_csr_permute_gpu": (C.c_int, [P, _u32p, P]),
             "gb_pick_sources_gpu": (C.c_int, [P, C.c_int, C.c_uint64, C.c_int, _u32p, C.POINTER(C.c_int)]),
+            "gb_csr_from_snap_gpu": (C.c_int, [C.c_char_p, C.c_int, C.c_uint64, P, C.POINTER(_ConvertStats)]),
+            "gb_convert_snap_gpu": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(_ConvertStats)]),
             "gb_random_perm": (C.c_int, [C.c_uint64, C.c_uint64, _u32p]),
             "gb_gen_path": (C.c_int, [C.c_uint32, P]),
             "gb_gen_star": (C.c_int, [C.c_uint32, P]),
@@ -324,6 +334,21 @@ def symmetrize_gpu(g: Graph) -> Graph:
 
 def permute_gpu(g: Graph, perm) -> Graph:
     return _make(lib().gb_csr_permute_gpu, C.byref(g._c()), np.ascontiguousarray(perm, np.uint32))
+
+
+def from_snap_gpu(path: str, directed: bool, chunk_bytes: int = 0) -> tuple[Graph, dict]:
+    """SNAP edge-list text (plain or gzip) -> (CSR, stats), parsed on the GPU
+    (graph::convertSnap without the file write, src/graph/snap.cpp:85-149)."""
+    st, out = _ConvertStats(), _Csr()
+    check(lib().gb_csr_from_snap_gpu(os.fsencode(path), int(directed), chunk_bytes, C.byref(out), C.byref(st)))
+    return _take(out), st.as_dict()
+
+
+def convert_snap_gpu(in_path: str, out_path: str, directed: bool) -> dict:
+    """gconvert: SNAP text -> .bin (src/graph/convert.cpp:11-45); returns the stats."""
+    st = _ConvertStats()
+    check(lib().gb_convert_snap_gpu(os.fsencode(in_path), os.fsencode(out_path), int(directed), C.byref(st)))
+    return st.as_dict()
 
 
 def random_perm(n: int, seed: int = 1) -> np.ndarray:

@@ -1,6 +1,6 @@
 """Builds the library in-tree: graph_analytics_applesilicon_b200/libgraphb200.so
-(every .cu / .cpp under csrc/, compiled by nvcc for sm_100a) and the gbench
-command-line driver bin/gbench.
+(every .cu / .cpp under csrc/, compiled by nvcc for sm_100a) and the command-line
+programs bin/gbench (benchmark + validation) and bin/gconvert (SNAP -> .bin).
 
     python -m graph_analytics_applesilicon_b200.build [--force] [--verbose]
 
@@ -22,6 +22,7 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libgraphb200.so")
 GBENCH = os.path.join(PKG, "bin", "gbench")
+PROGRAMS = ("gbench", "gconvert")  # csrc/<name>.cpp -> bin/<name>
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-fopenmp",
               "-I" + os.path.join(ROOT, "include"), "-I" + CSRC] + ARCH
@@ -67,22 +68,23 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(os.path.dirname(GBENCH), exist_ok=True)
     lib_srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
-    lib_srcs = [s for s in lib_srcs if not os.path.basename(s).startswith("gbench")]
+    lib_srcs = [s for s in lib_srcs if os.path.splitext(os.path.basename(s))[0] not in PROGRAMS]
     extra = ["-Xptxas", "-v"] if ptxas_info else []
     with cf.ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(lambda s: _compile(s, force or ptxas_info, verbose or ptxas_info, extra), lib_srcs))
     if force or _stale(LIB, objs):
-        cmd = [nvcc(), "-shared", "-o", LIB] + objs + ARCH + ["-Xcompiler", "-fopenmp", "-lgomp"]
+        cmd = [nvcc(), "-shared", "-o", LIB] + objs + ARCH + ["-Xcompiler", "-fopenmp", "-lgomp", "-lz"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    gb_src = os.path.join(CSRC, "gbench.cpp")
-    if os.path.exists(gb_src) and (force or _stale(GBENCH, [gb_src, LIB] + _headers())):
-        cmd = ["g++", "-std=c++17", "-O2", "-fopenmp", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, gb_src,
-               "-o", GBENCH, "-L" + PKG, "-lgraphb200", "-Wl,-rpath,$ORIGIN/.."]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"gbench build failed:\n{r.stdout}\n{r.stderr}")
+    for prog in PROGRAMS:
+        src, exe = os.path.join(CSRC, prog + ".cpp"), os.path.join(PKG, "bin", prog)
+        if os.path.exists(src) and (force or _stale(exe, [src, LIB] + _headers())):
+            cmd = ["g++", "-std=c++17", "-O2", "-fopenmp", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, src,
+                   "-o", exe, "-L" + PKG, "-lgraphb200", "-Wl,-rpath,$ORIGIN/.."]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"{prog} build failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

@@ -24,7 +24,7 @@
 
 #include "capi_util.hpp"
 #include "graph_host.hpp"
-#include "prims.cuh"
+#include "graph_prep.cuh"
 
 namespace gb {
 namespace {
@@ -239,19 +239,21 @@ __global__ void ccMaskKernel(uint64_t n, const uint32_t* parent, const unsigned 
         ok[v] = parent[v] == root ? 1 : 0;
 }
 
-uint32_t gridOf(uint64_t work, uint32_t threads) {
+}  // namespace
+
+uint32_t prepGrid(uint64_t work, uint32_t threads) {
     const uint64_t g = (work + threads - 1) / threads;
     return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(g, (uint64_t)deviceSmCount() * 16));
 }
 
-int bitsFor(uint64_t n) {
+int keyBits(uint64_t n) {
     int b = 1;
     while (b < 32 && (1ull << b) < n) ++b;
     return b;
 }
 
 // Sorts N keys whose used bits are [0, bits) in place (a holds the result).
-void radixSort(DevBuf<unsigned long long>& a, DevBuf<unsigned long long>& tmp, uint64_t N, int bits,
+void radixSortKeys(DevBuf<unsigned long long>& a, DevBuf<unsigned long long>& tmp, uint64_t N, int bits,
                ScanScratch& sc, cudaStream_t st) {
     if (N < 2) return;
     if (N >= (1ull << 32)) throw Error(GB_ERR_ARG, "graph prep: more than 2^32 entries");
@@ -286,10 +288,10 @@ void keysToCsr(DevBuf<unsigned long long>& keys, uint64_t N, uint64_t n, int b, 
     GB_CUDA(cudaMemsetAsync(deg.get(), 0, (n + 1) * 4, st));
     uint32_t m2 = 0;
     if (N) {
-        rsKeepKernel<<<gridOf(N, 256), 256, 0, st>>>(keys.get(), N, b, unique, dropSelf, keep.get());
+        rsKeepKernel<<<prepGrid(N, 256), 256, 0, st>>>(keys.get(), N, b, unique, dropSelf, keep.get());
         GB_LAUNCH_CHECK();
         scanExclusive(keep.get(), pos.get(), N, total.get(), sc, st);
-        rsEmitKernel<<<gridOf(N, 256), 256, 0, st>>>(keys.get(), N, b, keep.get(), pos.get(), col.get(), deg.get());
+        rsEmitKernel<<<prepGrid(N, 256), 256, 0, st>>>(keys.get(), N, b, keep.get(), pos.get(), col.get(), deg.get());
         GB_LAUNCH_CHECK();
         GB_CUDA(cudaMemcpyAsync(&m2, total.get(), 4, cudaMemcpyDeviceToHost, st));
     }
@@ -313,6 +315,8 @@ void keysToCsr(DevBuf<unsigned long long>& keys, uint64_t N, uint64_t n, int b, 
     out->row_ptr = hrp;
     out->col_idx = hci;
 }
+
+namespace {
 
 // Reads the device check word; throws if any check failed.
 void requireChecks(DevBuf<unsigned>& bad, cudaStream_t st) {
@@ -350,27 +354,27 @@ void csrOp(const gb_csr* g, int mode, const uint32_t* permHost, bool unique, boo
     bad.ensure(1);
     GB_CUDA(cudaMemsetAsync(bad.get(), 0, 4, st.s));
     uploadCsr(g, rp, ci, st.s);
-    checkCsrKernel<<<gridOf(std::max(g->n, g->m), 256), 256, 0, st.s>>>(rp.get(), ci.get(), g->n, g->m, bad.get());
+    checkCsrKernel<<<prepGrid(std::max(g->n, g->m), 256), 256, 0, st.s>>>(rp.get(), ci.get(), g->n, g->m, bad.get());
     GB_LAUNCH_CHECK();
     if (mode == 2) {
         perm.ensure(g->n);
         seen.ensure((g->n + 31) / 32);
         GB_CUDA(cudaMemcpyAsync(perm.get(), permHost, g->n * 4, cudaMemcpyHostToDevice, st.s));
         GB_CUDA(cudaMemsetAsync(seen.get(), 0, (g->n + 31) / 32 * 4, st.s));
-        checkPermKernel<<<gridOf(g->n, 256), 256, 0, st.s>>>(perm.get(), g->n, seen.get(), bad.get());
+        checkPermKernel<<<prepGrid(g->n, 256), 256, 0, st.s>>>(perm.get(), g->n, seen.get(), bad.get());
         GB_LAUNCH_CHECK();
     }
     requireChecks(bad, st.s);
-    const int b = bitsFor(g->n);
+    const int b = keyBits(g->n);
     const uint64_t N = mode == 3 ? 2 * g->m : g->m;
     DevBuf<unsigned long long> keys, tmp;
     keys.ensure(N + 1);
     if (g->m) {
-        csrKeysKernel<<<gridOf(g->n * 32, 256), 256, 0, st.s>>>(rp.get(), ci.get(), g->n, g->m, b, mode, perm.get(),
+        csrKeysKernel<<<prepGrid(g->n * 32, 256), 256, 0, st.s>>>(rp.get(), ci.get(), g->n, g->m, b, mode, perm.get(),
                                                                  keys.get());
         GB_LAUNCH_CHECK();
     }
-    radixSort(keys, tmp, N, 2 * b, sc, st.s);
+    radixSortKeys(keys, tmp, N, 2 * b, sc, st.s);
     keysToCsr(keys, N, g->n, b, unique, dropSelf, flags, sc, st.s, out);
 }
 
@@ -397,19 +401,19 @@ int gb_csr_from_edges_gpu(uint64_t n, const uint32_t* eu, const uint32_t* ev, ui
         if (ne) {
             GB_CUDA(cudaMemcpyAsync(du.get(), eu, ne * 4, cudaMemcpyHostToDevice, st.s));
             GB_CUDA(cudaMemcpyAsync(dv.get(), ev, ne * 4, cudaMemcpyHostToDevice, st.s));
-            checkEdgesKernel<<<gridOf(ne, 256), 256, 0, st.s>>>(du.get(), dv.get(), ne, n, bad.get());
+            checkEdgesKernel<<<prepGrid(ne, 256), 256, 0, st.s>>>(du.get(), dv.get(), ne, n, bad.get());
             GB_LAUNCH_CHECK();
         }
         requireChecks(bad, st.s);
-        const int b = bitsFor(n);
+        const int b = keyBits(n);
         const uint64_t N = directed ? ne : 2 * ne;
         DevBuf<unsigned long long> keys, tmp;
         keys.ensure(N + 1);
         if (ne) {
-            edgeKeysKernel<<<gridOf(ne, 256), 256, 0, st.s>>>(du.get(), dv.get(), ne, b, !directed, keys.get());
+            edgeKeysKernel<<<prepGrid(ne, 256), 256, 0, st.s>>>(du.get(), dv.get(), ne, b, !directed, keys.get());
             GB_LAUNCH_CHECK();
         }
-        radixSort(keys, tmp, N, 2 * b, sc, st.s);
+        radixSortKeys(keys, tmp, N, 2 * b, sc, st.s);
         keysToCsr(keys, N, n, b, true, true, (directed ? kFlagDirected : 0u) | kFlagSorted | kFlagDedup, sc, st.s,
                   out);
     });
@@ -473,13 +477,13 @@ int gb_pick_sources_gpu(const gb_csr* g, int count, uint64_t seed, int any_compo
             best.ensure(1);
             GB_CUDA(cudaMemsetAsync(bad.get(), 0, 4, st.s));
             uploadCsr(g, rp, ci, st.s);
-            checkCsrKernel<<<gridOf(std::max(n, g->m), 256), 256, 0, st.s>>>(rp.get(), ci.get(), n, g->m, bad.get());
+            checkCsrKernel<<<prepGrid(std::max(n, g->m), 256), 256, 0, st.s>>>(rp.get(), ci.get(), n, g->m, bad.get());
             GB_LAUNCH_CHECK();
             requireChecks(bad, st.s);
             parent.ensure(n);
             size.ensure(n);
             dok.ensure(n);
-            initIotaKernel<<<gridOf(n, 256), 256, 0, st.s>>>(parent.get(), n);
+            initIotaKernel<<<prepGrid(n, 256), 256, 0, st.s>>>(parent.get(), n);
             GB_LAUNCH_CHECK();
             // hook + jump rounds; each round at least halves the number of
             // roots that still have a smaller neighbouring root, so 64 rounds
@@ -487,10 +491,10 @@ int gb_pick_sources_gpu(const gb_csr* g, int count, uint64_t seed, int any_compo
             bool done = false;
             for (int round = 0; round < 64 && !done; ++round) {
                 GB_CUDA(cudaMemsetAsync(changed.get(), 0, 4, st.s));
-                ccHookKernel<<<gridOf(n * 32, 256), 256, 0, st.s>>>(rp.get(), ci.get(), n, parent.get(),
+                ccHookKernel<<<prepGrid(n * 32, 256), 256, 0, st.s>>>(rp.get(), ci.get(), n, parent.get(),
                                                                       changed.get());
                 GB_LAUNCH_CHECK();
-                ccJumpKernel<<<gridOf(n, 256), 256, 0, st.s>>>(n, parent.get());
+                ccJumpKernel<<<prepGrid(n, 256), 256, 0, st.s>>>(n, parent.get());
                 GB_LAUNCH_CHECK();
                 unsigned h = 0;
                 GB_CUDA(cudaMemcpyAsync(&h, changed.get(), 4, cudaMemcpyDeviceToHost, st.s));
@@ -500,9 +504,9 @@ int gb_pick_sources_gpu(const gb_csr* g, int count, uint64_t seed, int any_compo
             if (!done) throw Error(GB_ERR_STATE, "gb_pick_sources_gpu: components did not settle in 64 rounds");
             GB_CUDA(cudaMemsetAsync(size.get(), 0, n * 4, st.s));
             GB_CUDA(cudaMemsetAsync(best.get(), 0, 8, st.s));
-            ccSizeKernel<<<gridOf(n, 256), 256, 0, st.s>>>(n, parent.get(), size.get());
-            ccBestKernel<<<gridOf(n, 256), 256, 0, st.s>>>(n, size.get(), best.get());
-            ccMaskKernel<<<gridOf(n, 256), 256, 0, st.s>>>(n, parent.get(), best.get(), dok.get());
+            ccSizeKernel<<<prepGrid(n, 256), 256, 0, st.s>>>(n, parent.get(), size.get());
+            ccBestKernel<<<prepGrid(n, 256), 256, 0, st.s>>>(n, size.get(), best.get());
+            ccMaskKernel<<<prepGrid(n, 256), 256, 0, st.s>>>(n, parent.get(), best.get(), dok.get());
             GB_LAUNCH_CHECK();
             GB_CUDA(cudaMemcpyAsync(ok.data(), dok.get(), n, cudaMemcpyDeviceToHost, st.s));
             GB_CUDA(cudaStreamSynchronize(st.s));

@@ -1,0 +1,24 @@
+// graph_prep.cuh -- the key-sort pipeline of graph_prep.cu, shared with the
+// SNAP edge-list converter (snap_gpu.cu): 64-bit (row << b | column) keys,
+// stable LSD radix sort, then keys -> CSR.
+#pragma once
+
+#include "graph_b200.h"
+#include "prims.cuh"
+
+namespace gb {
+
+// Blocks for a grid-stride loop over `work` items (at most 16 per SM).
+uint32_t prepGrid(uint64_t work, uint32_t threads);
+// Bits of the largest id below n (at least 1): the column field of a key.
+int keyBits(uint64_t n);
+// Sorts N keys whose used bits are [0, bits) in place (a holds the result;
+// tmp is scratch of N keys).  N < 2^32.
+void radixSortKeys(DevBuf<unsigned long long>& a, DevBuf<unsigned long long>& tmp, uint64_t N, int bits,
+                   ScanScratch& sc, cudaStream_t st);
+// Sorted keys -> host CSR in *out (n rows, b column bits), dropping repeated
+// keys (unique) and self-loops (dropSelf); out->flags = flags.
+void keysToCsr(DevBuf<unsigned long long>& keys, uint64_t N, uint64_t n, int b, bool unique, bool dropSelf,
+               uint32_t flags, ScanScratch& sc, cudaStream_t st, gb_csr* out);
+
+}  // namespace gb

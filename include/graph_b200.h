@@ -86,6 +86,31 @@ int gb_csr_permute_gpu(const gb_csr* g, const uint32_t* perm, gb_csr* out);
  * same sources as gb_pick_sources.  Symmetric graphs only. */
 int gb_pick_sources_gpu(const gb_csr* g, int count, uint64_t seed, int any_component, uint32_t* out,
                         int* k);
+/* SNAP edge list (plain text or gzip) -> CSR, parsed and compacted on the
+ * GPU: graph::convertSnap (src/graph/snap.cpp:85-149, ConvertStats in
+ * src/graph/snap.hpp:9-16) with the line rules of forEachEdge (:17-81):
+ * '#' / '%' comment lines, blank lines, ' ' / '\t' separators, '\r' before a
+ * line's text, extra columns ignored; ids relabelled densely in increasing
+ * raw-id order; undirected (directed = 0) adds both directions; lists sorted,
+ * duplicates and self-loops dropped; flags Sorted | Dedup (| Directed).
+ * Errors (GB_ERR_ARG, the reference's messages): "<path>: malformed line N",
+ * "<path>: vertex ID too large on line N", "line longer than 4 MB in <path>"
+ * (first failing line in file order), "too many edges for uint32 offsets";
+ * GB_ERR_IO: "cannot open <path>", "gzread failed on <path>".
+ * chunk_bytes: text bytes per device chunk (0 = 64 MiB; at least 4 MiB + 1). */
+typedef struct {
+    uint64_t lines;      /* edge lines parsed */
+    uint64_t raw_max_id; /* largest raw id (0 when there are no edges) */
+    uint64_t n;          /* vertices after relabelling */
+    uint64_t m_before;   /* entries before duplicate / self-loop removal */
+    uint64_t m;          /* entries of the result */
+    double seconds;
+} gb_convert_stats;
+int gb_csr_from_snap_gpu(const char* path, int directed, uint64_t chunk_bytes, gb_csr* out,
+                         gb_convert_stats* stats);
+/* The converter of gconvert (src/graph/convert.cpp:11-45): text -> .bin. */
+int gb_convert_snap_gpu(const char* in_path, const char* out_path, int directed,
+                        gb_convert_stats* stats);
 /* reorder::compute(..., "random", seed) (src/graph/reorder.cpp:20-25). */
 int gb_random_perm(uint64_t n, uint64_t seed, uint32_t* perm);
 

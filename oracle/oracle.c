@@ -11,8 +11,10 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <zlib.h>
 
 /* ------------------------------------------------------------------ utils */
 
@@ -732,4 +734,141 @@ void orc_mlp_forward(int nf, int nh, int no, const float* P, int batch, const fl
     }
     free(h1);
     free(h2);
+}
+
+/* ------------------------------------------------------------ SNAP text */
+
+/* The whole (decompressed) file; gzread passes plain text through unchanged. */
+static char* read_all(const char* path, uint64_t* len, int* io_err) {
+    gzFile f = gzopen(path, "rb");
+    *io_err = 0;
+    if (!f) {
+        *io_err = 1;
+        return NULL;
+    }
+    uint64_t cap = 1 << 20, n = 0;
+    char* buf = (char*)xmalloc(cap);
+    for (;;) {
+        if (cap - n < (1 << 20)) {
+            cap *= 2;
+            buf = (char*)realloc(buf, cap);
+            if (!buf) abort();
+        }
+        int got = gzread(f, buf + n, (unsigned)(cap - n > (1u << 30) ? (1u << 30) : cap - n));
+        if (got < 0) {
+            *io_err = 2;
+            break;
+        }
+        if (got == 0) break;
+        n += (uint64_t)got;
+    }
+    gzclose(f);
+    *len = n;
+    return buf;
+}
+
+static int cmp_u32_snap(const void* a, const void* b) {
+    uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
+    return x < y ? -1 : x > y;
+}
+
+/* src/graph/snap.cpp:17-81 (forEachEdge: the line rules and the errors, one
+ * line at a time; a line of 4 MiB or more before its newline is the
+ * reference's "longer than 4 MB" case of its 4 MiB read buffer) and
+ * src/graph/snap.cpp:85-149 (convertSnap: dense relabelling in raw-id order,
+ * then fromEdgeList's count / scatter / compact). */
+int orc_convert_snap(const char* path, int directed, orc_csr** out, orc_convert_stats* st,
+                     char* msg, size_t cap) {
+    const uint64_t kLongLine = 4u << 20;
+    int io = 0;
+    uint64_t len = 0;
+    char* t = read_all(path, &len, &io);
+    *out = NULL;
+    memset(st, 0, sizeof *st);
+    if (io == 1) {
+        snprintf(msg, cap, "cannot open %s", path);
+        return 1;
+    }
+    if (io == 2) {
+        free(t);
+        snprintf(msg, cap, "gzread failed on %s", path);
+        return 1;
+    }
+    edge_list e = {0};
+    uint64_t line_no = 0, pos = 0;
+    int bad = 0;
+    while (pos < len && !bad) {
+        uint64_t end = pos;
+        while (end < len && t[end] != '\n') ++end; /* [pos, end): this line */
+        ++line_no;
+        if (end - pos >= kLongLine) {
+            snprintf(msg, cap, "line longer than 4 MB in %s", path);
+            bad = 1;
+            break;
+        }
+        uint64_t p = pos;
+        const uint64_t next = end + 1;
+        pos = next;
+        while (p < end && (t[p] == ' ' || t[p] == '\t' || t[p] == '\r')) ++p;
+        if (p == end || t[p] == '#' || t[p] == '%') continue; /* blank or comment */
+        uint64_t ids[2];
+        for (int k = 0; k < 2; ++k) {
+            while (p < end && (t[p] == ' ' || t[p] == '\t')) ++p;
+            if (p == end || t[p] < '0' || t[p] > '9') {
+                snprintf(msg, cap, "%s: malformed line %llu", path, (unsigned long long)line_no);
+                bad = 1;
+                break;
+            }
+            uint64_t x = 0; /* wraps modulo 2^64 like the reference's uint64_t */
+            while (p < end && t[p] >= '0' && t[p] <= '9') x = x * 10 + (uint64_t)(t[p++] - '0');
+            if (x >= 0xFFFFFFFFull) {
+                snprintf(msg, cap, "%s: vertex ID too large on line %llu", path,
+                         (unsigned long long)line_no);
+                bad = 1;
+                break;
+            }
+            ids[k] = x;
+        }
+        if (bad) break;
+        el_push(&e, (uint32_t)ids[0], (uint32_t)ids[1]);
+    }
+    free(t);
+    if (bad) {
+        free(e.u);
+        free(e.v);
+        return 1;
+    }
+    const uint64_t total = directed ? e.size : 2 * e.size;
+    st->lines = e.size;
+    st->m_before = total;
+    if (total >= 0xFFFFFFFFull) {
+        free(e.u);
+        free(e.v);
+        snprintf(msg, cap, "too many edges for uint32 offsets");
+        return 1;
+    }
+    /* distinct raw ids in increasing order; dense id = rank */
+    uint32_t* ids = (uint32_t*)xmalloc(2 * e.size * sizeof(uint32_t));
+    for (uint64_t i = 0; i < e.size; ++i) {
+        ids[2 * i] = e.u[i];
+        ids[2 * i + 1] = e.v[i];
+    }
+    qsort(ids, 2 * e.size, sizeof(uint32_t), cmp_u32_snap);
+    uint64_t n = 0;
+    for (uint64_t i = 0; i < 2 * e.size; ++i)
+        if (i == 0 || ids[i] != ids[i - 1]) ids[n++] = ids[i];
+    for (uint64_t i = 0; i < e.size; ++i) {
+        uint32_t* a = (uint32_t*)bsearch(&e.u[i], ids, n, sizeof(uint32_t), cmp_u32_snap);
+        uint32_t* b = (uint32_t*)bsearch(&e.v[i], ids, n, sizeof(uint32_t), cmp_u32_snap);
+        e.u[i] = (uint32_t)(a - ids);
+        e.v[i] = (uint32_t)(b - ids);
+    }
+    st->raw_max_id = n ? ids[n - 1] : 0;
+    st->n = n;
+    free(ids);
+    *out = orc_from_edge_list(n, e.u, e.v, e.size, directed);
+    st->m = (*out)->m;
+    free(e.u);
+    free(e.v);
+    return 0;
 }

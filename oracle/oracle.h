@@ -16,6 +16,7 @@
 #ifndef GRAPH_ORACLE_H
 #define GRAPH_ORACLE_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -95,6 +96,19 @@ void orc_check_ranks_f64(const double* ref, const double* got, uint64_t n, doubl
                          double* max_rel_top, double* sum);
 /* gsNoWorseThanJacobi (src/cpu/pagerank_cpu.hpp:80-84). */
 int orc_gs_no_worse(double gs_l1, double gs_rel, double gs_sum, double j_l1, double j_rel);
+
+/* SNAP edge list (plain or gzip text) -> CSR (src/graph/snap.cpp:17-149).
+ * Lines: blank or whitespace-only lines and lines whose first non-blank byte
+ * is '#' or '%' are skipped; otherwise two decimal ids separated by spaces or
+ * tabs, anything after the second id ignored.  Ids are relabelled densely in
+ * increasing raw-id order; directed = 0 adds both directions; lists sorted,
+ * duplicates and self-loops dropped.  Returns 0, or 1 with the reference's
+ * error message in msg (the first failing line in file order wins). */
+typedef struct {
+    uint64_t lines, raw_max_id, n, m_before, m;
+} orc_convert_stats;
+int orc_convert_snap(const char* path, int directed, orc_csr** out, orc_convert_stats* st,
+                     char* msg, size_t cap);
 
 /* Reference two-layer-ReLU MLP (forward, backward of the mean squared error)
  * used to check the GPU selector-training kernels.  Layout: w1[h][f], b1[h],

@@ -49,6 +49,10 @@ class _Csr(C.Structure):
                 ("row_ptr", C.POINTER(C.c_uint32)), ("col_idx", C.POINTER(C.c_uint32))]
 
 
+class _ConvertStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("lines", "raw_max_id", "n", "m_before", "m")]
+
+
 class _Level(C.Structure):
     _fields_ = [("level", C.c_uint32), ("direction", C.c_uint32),
                 ("frontier", C.c_uint64), ("edges", C.c_uint64)]
@@ -115,6 +119,9 @@ def lib():
                                         _f32p, _f32p]
         L.orc_mlp_loss_grad.restype = C.c_double
         L.orc_mlp_forward.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, C.c_int, _f32p, _f32p]
+        L.orc_convert_snap.argtypes = [C.c_char_p, C.c_int, C.POINTER(P), C.POINTER(_ConvertStats),
+                                       C.c_char_p, C.c_size_t]
+        L.orc_convert_snap.restype = C.c_int
         _orc = L
     return _orc
 
@@ -277,6 +284,21 @@ def mlp_forward(nf, nh, no, params, x):
     return out
 
 
+class ConvertError(RuntimeError):
+    """A converter failure; str() is the reference's message."""
+
+
+def convert_snap(path: str, directed: bool) -> tuple[HostGraph, dict]:
+    """SNAP text (plain or gzip) -> (CSR, stats) by the oracle; raises
+    ConvertError with the reference's message on bad input."""
+    out = C.POINTER(_Csr)()
+    st = _ConvertStats()
+    msg = C.create_string_buffer(1024)
+    if lib().orc_convert_snap(path.encode(), int(directed), C.byref(out), C.byref(st), msg, 1024):
+        raise ConvertError(msg.value.decode())
+    return _take(out), {k: int(getattr(st, k)) for k, _ in _ConvertStats._fields_}
+
+
 # --------------------------------------------------- the reference's own code
 
 _ref = None
@@ -323,6 +345,8 @@ def ref():
         L.gref_pagerank.restype = C.c_int
         L.gref_check_ranks_f32.argtypes = [_f64p, _f32p, C.c_uint64] + [C.POINTER(C.c_double)] * 3
         L.gref_max_threads.restype = C.c_int
+        L.gref_convert_snap.argtypes = [C.c_char_p, C.c_char_p, C.c_int, _u64p, C.c_char_p, C.c_size_t]
+        L.gref_convert_snap.restype = vp
         _ref = L
     return _ref
 
@@ -401,3 +425,15 @@ class RefGraph:
 
 def ref_suite(name: str) -> RefGraph:
     return RefGraph(ref().gref_suite(name.encode()))
+
+
+def ref_convert_snap(path: str, out_path: str, directed: bool) -> tuple[RefGraph, dict]:
+    """graph::convertSnap(path, out_path, directed), then graph::load(out_path);
+    raises ConvertError with the reference's exception text."""
+    st = np.zeros(5, np.uint64)
+    msg = C.create_string_buffer(1024)
+    h = ref().gref_convert_snap(path.encode(), out_path.encode(), int(directed), st, msg, 1024)
+    if not h:
+        raise ConvertError(msg.value.decode())
+    keys = ("lines", "raw_max_id", "n", "m_before", "m")
+    return RefGraph(h), {k: int(v) for k, v in zip(keys, st)}

@@ -2,7 +2,7 @@
 //
 // TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file together with
 // the reference's unmodified sources (src/cpu/{bfs_cpu,pagerank_cpu}.cpp,
-// src/graph/{csr,transform,generators,reorder}.cpp, read in place) into
+// src/graph/{csr,transform,generators,reorder,snap}.cpp, read in place) into
 // oracle/_ref/libgref.so.  Tests use it to pin the C restatement in oracle.c,
 // tests/golden/make_golden.py uses it to write the golden fixtures, and
 // bench.py times it as the CPU baseline (cpu_do / cpu_omp on all host cores).
@@ -12,10 +12,12 @@
 #include "graph/csr.hpp"
 #include "graph/generators.hpp"
 #include "graph/reorder.hpp"
+#include "graph/snap.hpp"
 #include "graph/transform.hpp"
 
 #include <omp.h>
 
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -119,6 +121,25 @@ void gref_check_ranks_f32(const double* ref, const float* got, uint64_t n, doubl
     *l1 = c.l1;
     *rel = c.maxRelTop;
     *sum = c.sum;
+}
+
+// graph::convertSnap then graph::load of its output.  Returns the loaded
+// graph, or null with the exception's text in msg.  stats: lines, raw_max_id,
+// n, m_before, m.
+void* gref_convert_snap(const char* in, const char* out, int directed, uint64_t* stats, char* msg,
+                        size_t cap) {
+    try {
+        graph::ConvertStats st = graph::convertSnap(in, out, directed != 0);
+        stats[0] = st.lines;
+        stats[1] = st.raw_max_id;
+        stats[2] = st.n;
+        stats[3] = st.m_before;
+        stats[4] = st.m;
+        return wrap(graph::load(out));
+    } catch (const std::exception& e) {
+        std::snprintf(msg, cap, "%s", e.what());
+        return nullptr;
+    }
 }
 
 }  // extern "C"

@@ -10,6 +10,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 GOLDEN_DIR = os.path.join(ROOT, "tests", "golden")
+sys.path.insert(0, GOLDEN_DIR)  # snap_cases
 
 
 def pytest_configure(config):
@@ -20,6 +21,12 @@ def pytest_configure(config):
 @pytest.fixture(scope="session")
 def golden():
     with open(os.path.join(GOLDEN_DIR, "golden.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="session")
+def snap_golden():
+    with open(os.path.join(GOLDEN_DIR, "snap_golden.json")) as f:
         return json.load(f)
 
 
