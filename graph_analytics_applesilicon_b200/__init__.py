@@ -132,6 +132,9 @@ def lib():
             "gb_csr_from_snap_gpu": (C.c_int, [C.c_char_p, C.c_int, C.c_uint64, P, C.POINTER(_ConvertStats)]),
             "gb_convert_snap_gpu": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(_ConvertStats)]),
             "gb_random_perm": (C.c_int, [C.c_uint64, C.c_uint64, _u32p]),
+            "gb_reorder": (C.c_int, [P, C.c_char_p, C.c_uint64, _u32p]),
+            "gb_reorder_gpu": (C.c_int, [P, C.c_char_p, C.c_uint64, _u32p]),
+            "gb_locality": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
             "gb_gen_path": (C.c_int, [C.c_uint32, P]),
             "gb_gen_star": (C.c_int, [C.c_uint32, P]),
             "gb_gen_complete": (C.c_int, [C.c_uint32, P]),
@@ -349,6 +352,27 @@ def convert_snap_gpu(in_path: str, out_path: str, directed: bool) -> dict:
     st = _ConvertStats()
     check(lib().gb_convert_snap_gpu(os.fsencode(in_path), os.fsencode(out_path), int(directed), C.byref(st)))
     return st.as_dict()
+
+
+def reorder(g: Graph, ordering: str, seed: int = 1) -> np.ndarray:
+    """reorder::compute on a symmetric graph (host): perm[old] = new."""
+    p = np.zeros(max(g.n, 1), np.uint32)
+    check(lib().gb_reorder(C.byref(g._c()), ordering.encode(), seed, p))
+    return p[: g.n]
+
+
+def reorder_gpu(g: Graph, ordering: str, seed: int = 1) -> np.ndarray:
+    """reorder with "degree" / "rcm" computed on the GPU (same permutation)."""
+    p = np.zeros(max(g.n, 1), np.uint32)
+    check(lib().gb_reorder_gpu(C.byref(g._c()), ordering.encode(), seed, p))
+    return p[: g.n]
+
+
+def locality(g: Graph) -> tuple[float, float]:
+    """(mean |u - v|, fraction of entries within one 64-vertex block)."""
+    a, b = C.c_double(0), C.c_double(0)
+    check(lib().gb_locality(C.byref(g._c()), C.byref(a), C.byref(b)))
+    return a.value, b.value
 
 
 def random_perm(n: int, seed: int = 1) -> np.ndarray:

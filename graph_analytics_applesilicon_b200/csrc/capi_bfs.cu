@@ -80,6 +80,7 @@ int gb_device_info(char* name, size_t cap, int* sm_count, int* cc_major, int* cc
         if (sm_count) *sm_count = p.multiProcessorCount;
         if (cc_major) *cc_major = p.major;
         if (cc_minor) *cc_minor = p.minor;
+        GB_CUDA(cudaFree(nullptr));  // creates the context now rather than inside the first timed call
     });
 }
 
@@ -137,6 +138,23 @@ int gb_random_perm(uint64_t n, uint64_t seed, uint32_t* perm) {
         GB_REQUIRE(perm || n == 0, "null output");
         auto p = randomPerm(n, seed);
         if (n) std::memcpy(perm, p.data(), n * 4);
+    });
+}
+
+int gb_reorder(const gb_csr* g, const char* ordering, uint64_t seed, uint32_t* perm) {
+    return guard([&] {
+        GB_REQUIRE(g && ordering && (perm || g->n == 0), "null argument");
+        const std::string o = ordering;
+        if (o != "original" && o != "random")
+            GB_REQUIRE(!(g->flags & 1u), "gb_reorder: orderings are computed on a symmetric graph");
+        auto p = orderingPerm(fromC(g), o, seed);
+        if (g->n) std::memcpy(perm, p.data(), g->n * 4);
+    });
+}
+int gb_locality(const gb_csr* g, double* mean_gap, double* same_block64) {
+    return guard([&] {
+        GB_REQUIRE(g && mean_gap && same_block64, "null argument");
+        locality(fromC(g), mean_gap, same_block64);
     });
 }
 

@@ -113,6 +113,9 @@ int prepTranspose(const gb_csr* g, gb_csr* out) {
 int prepPermute(const gb_csr* g, const uint32_t* perm, gb_csr* out) {
     return gHostPrep ? gb_csr_permute(g, perm, out) : gb_csr_permute_gpu(g, perm, out);
 }
+int prepReorder(const gb_csr* g, const char* ordering, uint64_t seed, uint32_t* perm) {
+    return gHostPrep ? gb_reorder(g, ordering, seed, perm) : gb_reorder_gpu(g, ordering, seed, perm);
+}
 int prepPickSources(const gb_csr* g, int count, uint64_t seed, int any, uint32_t* out, int* k) {
     return (gHostPrep || (g->flags & 1u)) ? gb_pick_sources(g, count, seed, any, out, k)
                                           : gb_pick_sources_gpu(g, count, seed, any, out, k);
@@ -380,6 +383,58 @@ std::string exeDir() {
 const std::vector<std::string> kVariants = {"cpu_serial", "cpu_omp", "cpu_do", "gpu_vertex", "gpu_naive",
                                             "gpu_binned", "gpu_edge", "gpu_do", "gpu_do_persistent", "hybrid"};
 
+// Keep the header and every row whose first field is not key, then append row
+// (the reference's util::csvUpsert, src/util/csv.hpp:18-37).
+void csvUpsert(const std::string& path, const std::string& header, const std::string& key, const std::string& row) {
+    std::vector<std::string> keep;
+    {
+        std::ifstream in(path);
+        std::string line;
+        bool first = true;
+        while (std::getline(in, line)) {
+            if (first) {
+                first = false;
+                continue;
+            }
+            if (!line.empty() && line.substr(0, line.find(',')) != key) keep.push_back(line);
+        }
+    }
+    std::ofstream out(path, std::ios::trunc);
+    out << header << '\n';
+    for (auto& l : keep) out << l << '\n';
+    out << row << '\n';
+}
+
+// --ordering original|random|degree|rcm: perm[old] = new computed on the
+// symmetric graph (empty for original); --locality-csv records the relabelled
+// graph's locality (src/bench/main.cpp:179-200).
+std::vector<uint32_t> orderingPerm(const Args& args, const Graph& sym, const std::string& dataset) {
+    const std::string ordering = args.get("ordering", "original");
+    std::vector<uint32_t> perm;
+    auto t0 = std::chrono::steady_clock::now();
+    if (ordering != "original") {
+        perm.resize(sym.n());
+        gpu::check(prepReorder(&sym.c, ordering.c_str(), (uint64_t)args.getInt("order-seed", 1), perm.data()));
+    }
+    const double orderMs = msSince(t0);
+    if (args.has("locality-csv")) {
+        Graph relabeled;
+        if (!perm.empty()) relabeled = make([&](gb_csr* o) { return prepPermute(&sym.c, perm.data(), o); });
+        const Graph& L = perm.empty() ? sym : relabeled;
+        double gap = 0, same = 0;
+        gpu::check(gb_locality(&L.c, &gap, &same));
+        char row[256];
+        std::snprintf(row, sizeof row, "%s/%s,%s,%s,%llu,%llu,%.2f,%.6f,%.0f", dataset.c_str(), ordering.c_str(),
+                      dataset.c_str(), ordering.c_str(), (unsigned long long)sym.n(), (unsigned long long)sym.m(), gap,
+                      same, orderMs);
+        csvUpsert(args.get("locality-csv"), "key,dataset,ordering,n,m_sym,mean_gap,same_block64,order_ms",
+                  dataset + "/" + ordering, row);
+        std::printf("locality (%s): mean |u-v| %.1f, same 64-block %.2f%%, ordering took %.0f ms\n", ordering.c_str(),
+                    gap, 100 * same, orderMs);
+    }
+    return perm;
+}
+
 int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
     const std::string variant = args.get("variant", "cpu_serial");
     if (std::find(kVariants.begin(), kVariants.end(), variant) == kVariants.end()) {
@@ -409,14 +464,8 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
 
     auto prep0 = std::chrono::steady_clock::now();
     Graph g = make([&](gb_csr* out) { return prepSymmetrize(&stored.c, out); });
-    std::vector<uint32_t> perm;
     const std::string ordering = args.get("ordering", "original");
-    if (ordering == "random") {
-        perm.resize(g.n());
-        gpu::check(gb_random_perm(g.n(), (uint64_t)args.getInt("order-seed", 1), perm.data()));
-    } else if (ordering != "original") {
-        throw std::runtime_error("ordering '" + ordering + "' is not supported (original | random)");
-    }
+    std::vector<uint32_t> perm = orderingPerm(args, g, dataset);
     Graph refG;  // original labels: sources, reference, TEPS denominators
     if (!perm.empty()) {
         refG = std::move(g);
@@ -677,31 +726,47 @@ int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
     const bool gsCheck = variant == "gpu_pull_gs" || o.inplace;
 
     auto prep0 = std::chrono::steady_clock::now();
-    Graph in = stored.directed() ? make([&](gb_csr* out) { return prepTranspose(&stored.c, out); })
-                                 : make([&](gb_csr* out) { return prepPermute(&stored.c, [&] {
-                                       static std::vector<uint32_t> id;
-                                       id.resize(stored.n());
-                                       std::iota(id.begin(), id.end(), 0u);
-                                       return id.data();
-                                   }(), out); });
-    std::vector<uint32_t> od(stored.n());
-    for (uint64_t v = 0; v < stored.n(); ++v) od[v] = stored.degree(v);
+    // --ordering: perm from the symmetric graph, applied to the stored graph
+    // (src/bench/main.cpp:459-500); ranks are reported in the original ids.
+    std::vector<uint32_t> perm;
+    if (args.get("ordering", "original") != "original" || args.has("locality-csv")) {
+        if (stored.directed()) {
+            Graph sym = make([&](gb_csr* out) { return prepSymmetrize(&stored.c, out); });
+            perm = orderingPerm(args, sym, dataset);
+        } else {
+            perm = orderingPerm(args, stored, dataset);
+        }
+    }
+    const bool permuted = !perm.empty();
+    Graph relabeled;
+    if (permuted) relabeled = make([&](gb_csr* out) { return prepPermute(&stored.c, perm.data(), out); });
+    const Graph& G = permuted ? relabeled : stored;  // what the variant runs on
+    Graph inOwn;
+    if (G.directed()) inOwn = make([&](gb_csr* out) { return prepTranspose(&G.c, out); });
+    const Graph& in = G.directed() ? inOwn : G;
+    std::vector<uint32_t> od(G.n());
+    for (uint64_t v = 0; v < G.n(); ++v) od[v] = G.degree(v);
     std::vector<double> ref, refConv;
     PrCheck jacobiErr;
     int refIters = 0;
-    if (validate) {
+    if (validate) {  // the reference in the original ids
+        Graph inO;
+        if (permuted && stored.directed()) inO = make([&](gb_csr* out) { return prepTranspose(&stored.c, out); });
+        const Graph& RI = !permuted ? in : stored.directed() ? inO : stored;
+        std::vector<uint32_t> odO(stored.n());
+        for (uint64_t v = 0; v < stored.n(); ++v) odO[v] = stored.degree(v);
         double ld = 0;
-        refIters = cpuPagerank(in, od, ref, iters, tol, nt, &ld);
+        refIters = cpuPagerank(RI, odO, ref, iters, tol, nt, &ld);
         if (gsCheck) {
-            cpuPagerank(in, od, refConv, 1000, 1e-10, nt, &ld);
+            cpuPagerank(RI, odO, refConv, 1000, 1e-10, nt, &ld);
             jacobiErr = checkRanks(refConv, ref.data());
         }
     }
     std::unique_ptr<gpu::GpuPageRank> gpr;
     if (gpuVariant) {
         const bool needOut = variant == "gpu_push";
-        gpr = std::make_unique<gpu::GpuPageRank>(stored.n(), needOut ? stored.c.row_ptr : nullptr,
-                                                 needOut ? stored.c.col_idx : nullptr, stored.m(), in.c.row_ptr,
+        gpr = std::make_unique<gpu::GpuPageRank>(G.n(), needOut ? G.c.row_ptr : nullptr,
+                                                 needOut ? G.c.col_idx : nullptr, G.m(), in.c.row_ptr,
                                                  in.c.col_idx, in.m(), od);
         if (variant == "gpu_pull_adaptive") gpr->prepareAdaptive(o.small_max, o.large_min);
         if (variant == "gpu_pull_gs") gpr->prepareGS((uint32_t)args.getInt("gs-pairs", 2));
@@ -724,12 +789,15 @@ int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
         lastDelta = r.last_delta;
         return r.gpu_ms;
     };
-    auto ranksD = [&]() {
-        std::vector<double> out(stored.n());
-        if (!gpuVariant) return rcpu;
-        if (pv == gpu::PrVariant::PullF64) return gpr->ranks64();
-        const float* r = gpr->ranks();
-        for (uint64_t v = 0; v < stored.n(); ++v) out[v] = r[v];
+    auto ranksD = [&]() {  // original ids: rank of v = result[perm[v]]
+        std::vector<double> out(stored.n()), r64;
+        const float* r = nullptr;
+        if (gpuVariant && pv == gpu::PrVariant::PullF64) r64 = gpr->ranks64();
+        else if (gpuVariant) r = gpr->ranks();
+        for (uint64_t v = 0; v < stored.n(); ++v) {
+            const uint64_t x = permuted ? perm[v] : v;
+            out[v] = !gpuVariant ? rcpu[x] : r ? (double)r[x] : r64[x];
+        }
         return out;
     };
     const int warmup = (int)args.getInt("warmup", 2), trials = (int)args.getInt("trials", 5);
@@ -784,6 +852,7 @@ int main(int argc, char** argv) {
         return 2;
     }
     gHostPrep = args.has("host-prep");
+    gb_device_info(nullptr, 0, nullptr, nullptr, nullptr);  // context up front; CPU-only runs ignore a failure
     try {
         std::string dataset;
         Graph g = loadGraph(args.get("graph"), dataset);

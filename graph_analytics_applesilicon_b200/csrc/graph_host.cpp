@@ -192,6 +192,88 @@ std::vector<uint32_t> randomPerm(uint64_t n, uint64_t seed) {
     return p;
 }
 
+namespace {
+
+// Vertices sorted by (degree, id), ascending or by descending degree.
+std::vector<uint32_t> byDegree(const HostCsr& g, bool descending) {
+    std::vector<uint32_t> v(g.n);
+    std::iota(v.begin(), v.end(), 0u);
+    std::stable_sort(v.begin(), v.end(), [&](uint32_t a, uint32_t b) {
+        return descending ? g.degree(a) > g.degree(b) : g.degree(a) < g.degree(b);
+    });
+    return v;
+}
+
+// One Cuthill-McKee breadth-first pass (src/graph/reorder.cpp:40-62): from
+// start over unmarked vertices, each vertex's newly marked neighbours appended
+// in (degree, id) order.  Returns the index in out where the last level begins.
+size_t cuthillMcKee(const HostCsr& g, uint32_t start, std::vector<uint8_t>& mark, std::vector<uint32_t>& out,
+                    std::vector<uint32_t>& fresh) {
+    size_t head = out.size(), levelBegin = head;
+    out.push_back(start);
+    mark[start] = 1;
+    auto less = [&](uint32_t a, uint32_t b) { return g.degree(a) != g.degree(b) ? g.degree(a) < g.degree(b) : a < b; };
+    while (head < out.size()) {
+        levelBegin = head;
+        for (const size_t end = out.size(); head < end; ++head) {
+            const uint32_t u = out[head];
+            fresh.clear();
+            for (uint32_t i = g.row_ptr[u]; i < g.row_ptr[u + 1]; ++i)
+                if (!mark[g.col_idx[i]]) {
+                    mark[g.col_idx[i]] = 1;
+                    fresh.push_back(g.col_idx[i]);
+                }
+            std::sort(fresh.begin(), fresh.end(), less);
+            out.insert(out.end(), fresh.begin(), fresh.end());
+        }
+    }
+    return levelBegin;
+}
+
+}  // namespace
+
+std::vector<uint32_t> orderingPerm(const HostCsr& g, const std::string& ordering, uint64_t seed) {
+    std::vector<uint32_t> perm(g.n);
+    if (ordering == "original") {
+        std::iota(perm.begin(), perm.end(), 0u);
+    } else if (ordering == "random") {
+        perm = randomPerm(g.n, seed);
+    } else if (ordering == "degree") {  // src/graph/reorder.cpp:27-38
+        const auto order = byDegree(g, true);
+        for (uint64_t i = 0; i < g.n; ++i) perm[order[i]] = (uint32_t)i;
+    } else if (ordering == "rcm") {  // src/graph/reorder.cpp:64-92
+        std::vector<uint8_t> mark(g.n, 0), probe(g.n, 0);
+        std::vector<uint32_t> order, pass, fresh;
+        order.reserve(g.n);
+        for (uint32_t s : byDegree(g, false)) {
+            if (mark[s]) continue;
+            pass.clear();
+            const size_t last = cuthillMcKee(g, s, probe, pass, fresh);
+            uint32_t start = pass[last];
+            for (size_t i = last; i < pass.size(); ++i)
+                if (g.degree(pass[i]) < g.degree(start)) start = pass[i];
+            cuthillMcKee(g, start, mark, order, fresh);
+        }
+        for (uint64_t i = 0; i < g.n; ++i) perm[order[i]] = (uint32_t)(g.n - 1 - i);
+    } else {
+        throw Error(GB_ERR_ARG, "unknown ordering '" + ordering + "' (original|random|degree|rcm)");
+    }
+    return perm;
+}
+
+void locality(const HostCsr& g, double* meanGap, double* sameBlock64) {
+    double gap = 0;
+    uint64_t same = 0;
+    for (uint64_t u = 0; u < g.n; ++u)
+        for (uint32_t i = g.row_ptr[u]; i < g.row_ptr[u + 1]; ++i) {
+            const uint64_t w = g.col_idx[i];
+            gap += (double)(u > w ? u - w : w - u);
+            same += (u >> 6) == (w >> 6);
+        }
+    *meanGap = g.m ? gap / (double)g.m : 0.0;
+    *sameBlock64 = g.m ? (double)same / (double)g.m : 0.0;
+}
+
 std::string csrValidate(const HostCsr& g) {
     if (g.m >= (1ull << 32)) return "m does not fit in uint32";
     if (g.row_ptr.size() != g.n + 1) return "row_ptr must have n+1 entries";

@@ -37,6 +37,11 @@ HostCsr csrTranspose(const HostCsr& g);
 HostCsr csrSymmetrize(const HostCsr& g);
 HostCsr csrPermute(const HostCsr& g, const uint32_t* perm);
 std::vector<uint32_t> randomPerm(uint64_t n, uint64_t seed);
+// reorder::compute (src/graph/reorder.cpp:94-100) on a symmetric graph:
+// perm[old] = new for "original" | "random" | "degree" | "rcm".
+std::vector<uint32_t> orderingPerm(const HostCsr& sym, const std::string& ordering, uint64_t seed);
+// reorder::locality (src/graph/reorder.cpp:111-125).
+void locality(const HostCsr& g, double* meanGap, double* sameBlock64);
 std::string csrValidate(const HostCsr& g);
 
 HostCsr genPath(uint32_t n);

@@ -254,11 +254,12 @@ int keyBits(uint64_t n) {
 
 // Sorts N keys whose used bits are [0, bits) in place (a holds the result).
 void radixSortKeys(DevBuf<unsigned long long>& a, DevBuf<unsigned long long>& tmp, uint64_t N, int bits,
-               ScanScratch& sc, cudaStream_t st) {
+                   ScanScratch& sc, cudaStream_t st, DevBuf<uint32_t>* countsScratch) {
     if (N < 2) return;
     if (N >= (1ull << 32)) throw Error(GB_ERR_ARG, "graph prep: more than 2^32 entries");
     const uint32_t tiles = (uint32_t)((N + kRsTile - 1) / kRsTile);
-    DevBuf<uint32_t> counts;
+    DevBuf<uint32_t> own;
+    DevBuf<uint32_t>& counts = countsScratch ? *countsScratch : own;
     counts.ensure((uint64_t)tiles * 256 + 1);
     tmp.ensure(N);
     unsigned long long* src = a.get();
@@ -316,6 +317,29 @@ void keysToCsr(DevBuf<unsigned long long>& keys, uint64_t N, uint64_t n, int b, 
     out->col_idx = hci;
 }
 
+// Connected components of a symmetric device CSR: parent[v] = the smallest
+// vertex of v's component (hook + jump rounds; each round at least halves the
+// number of roots that still have a smaller neighbouring root, so 64 rounds
+// cover any n < 2^32 many times over).
+void connectedComponents(const uint32_t* rp, const uint32_t* ci, uint64_t n, uint32_t* parent, cudaStream_t st) {
+    DevBuf<unsigned> changed;
+    changed.ensure(1);
+    initIotaKernel<<<prepGrid(n, 256), 256, 0, st>>>(parent, n);
+    GB_LAUNCH_CHECK();
+    for (int round = 0; round < 64; ++round) {
+        GB_CUDA(cudaMemsetAsync(changed.get(), 0, 4, st));
+        ccHookKernel<<<prepGrid(n * 32, 256), 256, 0, st>>>(rp, ci, n, parent, changed.get());
+        GB_LAUNCH_CHECK();
+        ccJumpKernel<<<prepGrid(n, 256), 256, 0, st>>>(n, parent);
+        GB_LAUNCH_CHECK();
+        unsigned h = 0;
+        GB_CUDA(cudaMemcpyAsync(&h, changed.get(), 4, cudaMemcpyDeviceToHost, st));
+        GB_CUDA(cudaStreamSynchronize(st));
+        if (h == 0) return;
+    }
+    throw Error(GB_ERR_STATE, "connected components did not settle in 64 rounds");
+}
+
 namespace {
 
 // Reads the device check word; throws if any check failed.
@@ -336,6 +360,24 @@ void uploadCsr(const gb_csr* g, DevBuf<uint32_t>& rp, DevBuf<uint32_t>& ci, cuda
     GB_CUDA(cudaMemcpyAsync(rp.get(), g->row_ptr, (g->n + 1) * 4, cudaMemcpyHostToDevice, st));
     if (g->m) GB_CUDA(cudaMemcpyAsync(ci.get(), g->col_idx, g->m * 4, cudaMemcpyHostToDevice, st));
 }
+
+}  // namespace
+
+void uploadCheckedCsr(const gb_csr* g, DevBuf<uint32_t>& rp, DevBuf<uint32_t>& ci, cudaStream_t st) {
+    GB_REQUIRE(g && g->row_ptr && (g->m == 0 || g->col_idx), "null CSR arrays");
+    GB_REQUIRE(g->n >= 1 && g->n < 0xFFFFFFFFull, "graph prep: n must be in [1, 2^32 - 1)");
+    GB_REQUIRE(g->m < (1ull << 32), "graph prep: m must fit in uint32");
+    GB_REQUIRE(g->row_ptr[0] == 0 && g->row_ptr[g->n] == g->m, "graph prep: row_ptr must run from 0 to m");
+    DevBuf<unsigned> bad;
+    bad.ensure(1);
+    GB_CUDA(cudaMemsetAsync(bad.get(), 0, 4, st));
+    uploadCsr(g, rp, ci, st);
+    checkCsrKernel<<<prepGrid(std::max(g->n, g->m), 256), 256, 0, st>>>(rp.get(), ci.get(), g->n, g->m, bad.get());
+    GB_LAUNCH_CHECK();
+    requireChecks(bad, st);
+}
+
+namespace {
 
 constexpr uint32_t kFlagDirected = 1u, kFlagSorted = 2u, kFlagDedup = 4u;
 
@@ -469,39 +511,14 @@ int gb_pick_sources_gpu(const gb_csr* g, int count, uint64_t seed, int any_compo
                        "out-edges of directed ones)");
             Stream st;
             DevBuf<uint32_t> rp, ci, parent, size;
-            DevBuf<unsigned> bad, changed;
             DevBuf<unsigned long long> best;
             DevBuf<uint8_t> dok;
-            bad.ensure(1);
-            changed.ensure(1);
             best.ensure(1);
-            GB_CUDA(cudaMemsetAsync(bad.get(), 0, 4, st.s));
-            uploadCsr(g, rp, ci, st.s);
-            checkCsrKernel<<<prepGrid(std::max(n, g->m), 256), 256, 0, st.s>>>(rp.get(), ci.get(), n, g->m, bad.get());
-            GB_LAUNCH_CHECK();
-            requireChecks(bad, st.s);
+            uploadCheckedCsr(g, rp, ci, st.s);
             parent.ensure(n);
             size.ensure(n);
             dok.ensure(n);
-            initIotaKernel<<<prepGrid(n, 256), 256, 0, st.s>>>(parent.get(), n);
-            GB_LAUNCH_CHECK();
-            // hook + jump rounds; each round at least halves the number of
-            // roots that still have a smaller neighbouring root, so 64 rounds
-            // cover any n < 2^32 many times over
-            bool done = false;
-            for (int round = 0; round < 64 && !done; ++round) {
-                GB_CUDA(cudaMemsetAsync(changed.get(), 0, 4, st.s));
-                ccHookKernel<<<prepGrid(n * 32, 256), 256, 0, st.s>>>(rp.get(), ci.get(), n, parent.get(),
-                                                                      changed.get());
-                GB_LAUNCH_CHECK();
-                ccJumpKernel<<<prepGrid(n, 256), 256, 0, st.s>>>(n, parent.get());
-                GB_LAUNCH_CHECK();
-                unsigned h = 0;
-                GB_CUDA(cudaMemcpyAsync(&h, changed.get(), 4, cudaMemcpyDeviceToHost, st.s));
-                GB_CUDA(cudaStreamSynchronize(st.s));
-                done = h == 0;
-            }
-            if (!done) throw Error(GB_ERR_STATE, "gb_pick_sources_gpu: components did not settle in 64 rounds");
+            connectedComponents(rp.get(), ci.get(), n, parent.get(), st.s);
             GB_CUDA(cudaMemsetAsync(size.get(), 0, n * 4, st.s));
             GB_CUDA(cudaMemsetAsync(best.get(), 0, 8, st.s));
             ccSizeKernel<<<prepGrid(n, 256), 256, 0, st.s>>>(n, parent.get(), size.get());

@@ -14,11 +14,19 @@ uint32_t prepGrid(uint64_t work, uint32_t threads);
 int keyBits(uint64_t n);
 // Sorts N keys whose used bits are [0, bits) in place (a holds the result;
 // tmp is scratch of N keys).  N < 2^32.
+// countsScratch (optional) is reused for the digit histograms across calls.
 void radixSortKeys(DevBuf<unsigned long long>& a, DevBuf<unsigned long long>& tmp, uint64_t N, int bits,
-                   ScanScratch& sc, cudaStream_t st);
+                   ScanScratch& sc, cudaStream_t st, DevBuf<uint32_t>* countsScratch = nullptr);
 // Sorted keys -> host CSR in *out (n rows, b column bits), dropping repeated
 // keys (unique) and self-loops (dropSelf); out->flags = flags.
 void keysToCsr(DevBuf<unsigned long long>& keys, uint64_t N, uint64_t n, int b, bool unique, bool dropSelf,
                uint32_t flags, ScanScratch& sc, cudaStream_t st, gb_csr* out);
+
+// Uploads a host CSR and checks it on the device (row_ptr from 0 to m and
+// non-decreasing, every column below n); throws GB_ERR_ARG otherwise.
+void uploadCheckedCsr(const gb_csr* g, DevBuf<uint32_t>& rp, DevBuf<uint32_t>& ci, cudaStream_t st);
+// Connected components of a symmetric device CSR: parent[v] = the smallest
+// vertex of v's component.
+void connectedComponents(const uint32_t* rp, const uint32_t* ci, uint64_t n, uint32_t* parent, cudaStream_t st);
 
 }  // namespace gb

@@ -36,7 +36,8 @@ typedef enum {
 } gb_status;
 
 const char* gb_last_error(void);
-/* Library version and the device it will use (name, SM count). */
+/* The device the library will use (name, SM count, compute capability);
+ * also creates its CUDA context, so that later calls do not pay for it. */
 int gb_device_info(char* name, size_t cap, int* sm_count, int* cc_major, int* cc_minor);
 
 /* ------------------------------------------------------------ host graphs */
@@ -113,6 +114,17 @@ int gb_convert_snap_gpu(const char* in_path, const char* out_path, int directed,
                         gb_convert_stats* stats);
 /* reorder::compute(..., "random", seed) (src/graph/reorder.cpp:20-25). */
 int gb_random_perm(uint64_t n, uint64_t seed, uint32_t* perm);
+/* reorder::compute(sym, ordering, seed) (src/graph/reorder.cpp:94-100) on a
+ * symmetric graph: perm[old] = new for "original", "random" (seed),
+ * "degree" (descending degree, ties by id, :27-38) or "rcm" (reverse
+ * Cuthill-McKee per component, :40-92).  gb_reorder runs on the host,
+ * gb_reorder_gpu computes "degree" and "rcm" on the GPU (same permutation;
+ * "original" and "random" stay on the host).  Unknown names: GB_ERR_ARG. */
+int gb_reorder(const gb_csr* sym, const char* ordering, uint64_t seed, uint32_t* perm);
+int gb_reorder_gpu(const gb_csr* sym, const char* ordering, uint64_t seed, uint32_t* perm);
+/* reorder::locality (src/graph/reorder.cpp:111-125): mean |u - v| over the
+ * stored entries and the fraction with u / 64 == v / 64. */
+int gb_locality(const gb_csr* g, double* mean_gap, double* same_block64);
 
 /* Generators: src/graph/generators.cpp:8-75 (same graphs, byte for byte). */
 int gb_gen_path(uint32_t n, gb_csr* out);

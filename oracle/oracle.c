@@ -318,6 +318,115 @@ void orc_random_perm(uint64_t n, uint64_t seed, uint32_t* p) {
     }
 }
 
+/* Orderings of src/graph/reorder.cpp:30-90, on a symmetric graph. */
+static const orc_csr* g_sort_graph; /* qsort has no context argument */
+static uint32_t deg_of(const orc_csr* g, uint32_t v) { return g->row_ptr[v + 1] - g->row_ptr[v]; }
+
+static int cmp_deg_desc_id(const void* a, const void* b) {
+    uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
+    uint32_t dx = deg_of(g_sort_graph, x), dy = deg_of(g_sort_graph, y);
+    if (dx != dy) return dx > dy ? -1 : 1;
+    return x < y ? -1 : x > y;
+}
+
+static int cmp_deg_asc_id(const void* a, const void* b) {
+    uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
+    uint32_t dx = deg_of(g_sort_graph, x), dy = deg_of(g_sort_graph, y);
+    if (dx != dy) return dx < dy ? -1 : 1;
+    return x < y ? -1 : x > y;
+}
+
+/* degreePerm (reorder.cpp:27-38): new ids by descending degree, ties by id
+ * (a stable sort of the identity). */
+void orc_reorder_degree(const orc_csr* g, uint32_t* perm) {
+    uint32_t* order = (uint32_t*)xmalloc(g->n * sizeof(uint32_t) + 4);
+    for (uint64_t v = 0; v < g->n; ++v) order[v] = (uint32_t)v;
+    g_sort_graph = g;
+    qsort(order, g->n, sizeof(uint32_t), cmp_deg_desc_id);
+    for (uint64_t i = 0; i < g->n; ++i) perm[order[i]] = (uint32_t)i;
+    free(order);
+}
+
+/* cmBfs (reorder.cpp:40-62): breadth-first from start over unmarked
+ * vertices; each vertex's newly marked neighbours are appended sorted by
+ * (degree, id).  Appends to out[*len]; returns where the last level begins. */
+static uint64_t cm_bfs(const orc_csr* g, uint32_t start, uint8_t* mark, uint32_t* out, uint64_t* len,
+                       uint32_t* scratch) {
+    uint64_t head = *len, last = head;
+    out[(*len)++] = start;
+    mark[start] = 1;
+    g_sort_graph = g;
+    while (head < *len) {
+        const uint64_t level_end = *len;
+        last = head;
+        for (; head < level_end; ++head) {
+            const uint32_t u = out[head];
+            uint64_t k = 0;
+            for (uint32_t i = g->row_ptr[u]; i < g->row_ptr[u + 1]; ++i) {
+                const uint32_t w = g->col_idx[i];
+                if (!mark[w]) {
+                    mark[w] = 1;
+                    scratch[k++] = w;
+                }
+            }
+            qsort(scratch, k, sizeof(uint32_t), cmp_deg_asc_id);
+            memcpy(out + *len, scratch, k * sizeof(uint32_t));
+            *len += k;
+        }
+    }
+    return last;
+}
+
+/* rcmPerm (reorder.cpp:64-92): components in the order of their first vertex
+ * by (degree, id); per component one probe pass from that vertex, whose last
+ * level's first lowest-degree vertex starts the real pass; the whole order
+ * reversed at the end. */
+void orc_reorder_rcm(const orc_csr* g, uint32_t* perm) {
+    const uint64_t n = g->n;
+    uint32_t* by_degree = (uint32_t*)xmalloc(n * sizeof(uint32_t) + 4);
+    uint32_t* order = (uint32_t*)xmalloc(n * sizeof(uint32_t) + 4);
+    uint32_t* tmp = (uint32_t*)xmalloc(n * sizeof(uint32_t) + 4);
+    uint32_t* scratch = (uint32_t*)xmalloc(n * sizeof(uint32_t) + 4);
+    uint8_t* mark = (uint8_t*)calloc(n + 1, 1);
+    uint8_t* probe = (uint8_t*)calloc(n + 1, 1);
+    for (uint64_t v = 0; v < n; ++v) by_degree[v] = (uint32_t)v;
+    g_sort_graph = g;
+    qsort(by_degree, n, sizeof(uint32_t), cmp_deg_asc_id);
+    uint64_t len = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint32_t s = by_degree[i];
+        if (mark[s]) continue;
+        uint64_t tl = 0;
+        const uint64_t last = cm_bfs(g, s, probe, tmp, &tl, scratch);
+        uint32_t start = tmp[last];
+        for (uint64_t j = last; j < tl; ++j)
+            if (deg_of(g, tmp[j]) < deg_of(g, start)) start = tmp[j];
+        cm_bfs(g, start, mark, order, &len, scratch);
+    }
+    for (uint64_t i = 0; i < n; ++i) perm[order[i]] = (uint32_t)(n - 1 - i);
+    free(by_degree);
+    free(order);
+    free(tmp);
+    free(scratch);
+    free(mark);
+    free(probe);
+}
+
+/* locality (reorder.cpp:111-125): mean |u - v| over stored entries and the
+ * fraction with u / 64 == v / 64. */
+void orc_locality(const orc_csr* g, double* mean_gap, double* same_block64) {
+    double gap = 0;
+    uint64_t same = 0;
+    for (uint64_t u = 0; u < g->n; ++u)
+        for (uint32_t i = g->row_ptr[u]; i < g->row_ptr[u + 1]; ++i) {
+            const uint64_t w = g->col_idx[i];
+            gap += u > w ? (double)(u - w) : (double)(w - u);
+            same += (u >> 6) == (w >> 6);
+        }
+    *mean_gap = g->m ? gap / (double)g->m : 0;
+    *same_block64 = g->m ? (double)same / (double)g->m : 0;
+}
+
 /* src/graph/csr.cpp:86-104 */
 int orc_validate(const orc_csr* g) {
     if (g->m >= (1ull << 32)) return 1;

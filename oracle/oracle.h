@@ -70,6 +70,12 @@ orc_csr* orc_transpose(const orc_csr* g);
 orc_csr* orc_symmetrize(const orc_csr* g);
 orc_csr* orc_permute(const orc_csr* g, const uint32_t* perm);
 void orc_random_perm(uint64_t n, uint64_t seed, uint32_t* perm);
+/* Orderings on a symmetric graph (src/graph/reorder.cpp:27-99): perm[old] =
+ * new; "degree" = descending degree (ties by id), "rcm" = reverse
+ * Cuthill-McKee per component.  locality (:111-125). */
+void orc_reorder_degree(const orc_csr* g, uint32_t* perm);
+void orc_reorder_rcm(const orc_csr* g, uint32_t* perm);
+void orc_locality(const orc_csr* g, double* mean_gap, double* same_block64);
 /* Structural check (src/graph/csr.cpp:86-104): 0 if valid. */
 int orc_validate(const orc_csr* g);
 

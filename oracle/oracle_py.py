@@ -119,6 +119,9 @@ def lib():
                                         _f32p, _f32p]
         L.orc_mlp_loss_grad.restype = C.c_double
         L.orc_mlp_forward.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, C.c_int, _f32p, _f32p]
+        L.orc_reorder_degree.argtypes = [P, _u32p]
+        L.orc_reorder_rcm.argtypes = [P, _u32p]
+        L.orc_locality.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_convert_snap.argtypes = [C.c_char_p, C.c_int, C.POINTER(P), C.POINTER(_ConvertStats),
                                        C.c_char_p, C.c_size_t]
         L.orc_convert_snap.restype = C.c_int
@@ -284,6 +287,26 @@ def mlp_forward(nf, nh, no, params, x):
     return out
 
 
+def reorder(g: HostGraph, ordering: str, seed: int = 1) -> np.ndarray:
+    """reorder::compute (src/graph/reorder.cpp:94-100): perm[old] = new."""
+    if ordering == "original":
+        return np.arange(g.n, dtype=np.uint32)
+    if ordering == "random":
+        return random_perm(g.n, seed)
+    p = np.zeros(max(g.n, 1), np.uint32)
+    fn = {"degree": lib().orc_reorder_degree, "rcm": lib().orc_reorder_rcm}[ordering]
+    v = _View(g)
+    fn(v.ptr, p)
+    return p[: g.n]
+
+
+def locality(g: HostGraph) -> tuple[float, float]:
+    """(mean |u - v|, fraction of entries within one 64-vertex block)."""
+    a, b, v = C.c_double(0), C.c_double(0), _View(g)
+    lib().orc_locality(v.ptr, C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
 class ConvertError(RuntimeError):
     """A converter failure; str() is the reference's message."""
 
@@ -345,6 +368,7 @@ def ref():
         L.gref_pagerank.restype = C.c_int
         L.gref_check_ranks_f32.argtypes = [_f64p, _f32p, C.c_uint64] + [C.POINTER(C.c_double)] * 3
         L.gref_max_threads.restype = C.c_int
+        L.gref_locality.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.gref_convert_snap.argtypes = [C.c_char_p, C.c_char_p, C.c_int, _u64p, C.c_char_p, C.c_size_t]
         L.gref_convert_snap.restype = vp
         _ref = L
@@ -392,6 +416,11 @@ class RefGraph:
         p = np.zeros(max(n, 1), np.uint32)
         ref().gref_ordering(self.h, name.encode(), seed, p)
         return p[:n]
+
+    def locality(self) -> tuple[float, float]:
+        a, b = C.c_double(0), C.c_double(0)
+        ref().gref_locality(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
 
     def bfs_serial(self, src: int) -> np.ndarray:
         n = int(ref().gref_n(self.h))

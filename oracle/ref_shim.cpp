@@ -64,6 +64,11 @@ void gref_ordering(void* h, const char* ordering, uint64_t seed, uint32_t* out) 
     auto p = graph::reorder::compute(csr(h), ordering, seed);
     std::memcpy(out, p.data(), p.size() * 4);
 }
+void gref_locality(void* h, double* mean_gap, double* same_block64) {
+    graph::reorder::Locality l = graph::reorder::locality(csr(h));
+    *mean_gap = l.meanGap;
+    *same_block64 = l.sameBlock64;
+}
 uint64_t gref_n(void* h) { return csr(h).n; }
 uint64_t gref_m(void* h) { return csr(h).m; }
 uint32_t gref_flags(void* h) { return csr(h).flags; }

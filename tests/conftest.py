@@ -31,6 +31,12 @@ def snap_golden():
 
 
 @pytest.fixture(scope="session")
+def order_golden():
+    with open(os.path.join(GOLDEN_DIR, "order_golden.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="session")
 def golden_ranks():
     return dict(np.load(os.path.join(GOLDEN_DIR, "golden_ranks.npz")))
 

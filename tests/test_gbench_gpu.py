@@ -1,5 +1,5 @@
-"""gbench end to end on the GPU: graph preparation on the device (the default)
-against --host-prep on the same command line.  Both runs must validate against
+"""gbench end to end on the GPU: graph preparation (and --ordering degree /
+rcm) on the device (the default) against --host-prep on the same command line.  Both runs must validate against
 the serial CPU BFS / FP64 PageRank and write byte-identical distances and ranks
 with the same sources, the contract of the reference's gbench
 (bench/gbench.cpp: prep, source picking, --validate)."""
@@ -49,6 +49,14 @@ CASES = {
                            "--iters", "20", "--trials", "1"],
     "grid_pr": ["--graph", "synth:grid100x100", "--algo", "pr", "--variant", "gpu_pull_adaptive",
                 "--iters", "20", "--trials", "1"],
+    "rmat12_rcm_bfs": ["--graph", "synth:rmat12", "--algo", "bfs", "--variant", "gpu_do_persistent",
+                       "--ordering", "rcm", "--sources", "8", "--trials", "1"],
+    "grid_degree_bfs": ["--graph", "synth:grid100x100", "--algo", "bfs", "--variant", "gpu_do",
+                        "--ordering", "degree", "--sources", "4", "--trials", "1"],
+    "rmat12_directed_rcm_pr": ["--graph", "synth:rmat12_directed", "--algo", "pr", "--variant", "gpu_pull_adaptive",
+                               "--ordering", "rcm", "--iters", "20", "--trials", "1"],
+    "rmat12_directed_degree_gs": ["--graph", "synth:rmat12_directed", "--algo", "pr", "--variant", "gpu_pull_gs",
+                                  "--ordering", "degree", "--tol", "1e-6", "--trials", "1"],
 }
 
 
