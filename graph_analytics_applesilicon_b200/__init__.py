@@ -134,6 +134,7 @@ def lib():
             "gb_random_perm": (C.c_int, [C.c_uint64, C.c_uint64, _u32p]),
             "gb_reorder": (C.c_int, [P, C.c_char_p, C.c_uint64, _u32p]),
             "gb_reorder_gpu": (C.c_int, [P, C.c_char_p, C.c_uint64, _u32p]),
+            "gb_csr_hub_first_gpu": (C.c_int, [P, P]),
             "gb_locality": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
             "gb_gen_path": (C.c_int, [C.c_uint32, P]),
             "gb_gen_star": (C.c_int, [C.c_uint32, P]),
@@ -160,6 +161,7 @@ def lib():
             "gb_selector_shape": (C.c_int, [C.POINTER(C.c_int)] * 3),
             "gb_selector_param_count": (C.c_size_t, []),
             "gb_bfs_set_selector": (C.c_int, [vp, C.c_int, vp, C.c_size_t]),
+            "gb_bfs_hub_first": (C.c_int, [vp]),
             "gb_bfs_profile_levels": (C.c_int, [vp, C.c_uint32, C.POINTER(BfsOptions), C.c_int, _f32p, _f32p,
                                                 C.c_size_t, C.POINTER(C.c_size_t)]),
             "gb_bfs_profile_batch_levels": (C.c_int, [vp, _u32p, C.c_int, C.POINTER(BfsOptions), C.c_int, _f32p,
@@ -368,6 +370,11 @@ def reorder_gpu(g: Graph, ordering: str, seed: int = 1) -> np.ndarray:
     return p[: g.n]
 
 
+def hub_first_gpu(g: Graph) -> Graph:
+    """Adjacency lists by descending neighbour degree, ties by id (GPU)."""
+    return _make(lib().gb_csr_hub_first_gpu, C.byref(g._c()))
+
+
 def locality(g: Graph) -> tuple[float, float]:
     """(mean |u - v|, fraction of entries within one 64-vertex block)."""
     a, b = C.c_double(0), C.c_double(0)
@@ -479,6 +486,12 @@ class GpuBfs:
 
     def lastLevels(self) -> int:
         return lib().gb_bfs_last_levels(self._h)
+
+    def hub_first(self):
+        """Hub-first adjacency order on the device: same depths, bottom-up
+        levels exit earlier (trace edges of bottom-up levels follow it)."""
+        check(lib().gb_bfs_hub_first(self._h))
+        return self
 
     def set_selector(self, params, which: int = 0):
         if params is None:

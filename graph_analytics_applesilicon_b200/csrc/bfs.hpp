@@ -33,6 +33,7 @@ struct gb_bfs {
     uint64_t n = 0, m = 0;
     std::vector<uint32_t> hostRowPtr;  // degrees of sources on the host
     gb::DevBuf<uint32_t> rowPtr, colIdx, dist;
+    bool hubFirst = false;  // adjacency lists re-sorted hub-first (gb_bfs_hub_first)
     gb::Stream stream;
     gb::EventPair ev;
     gb::ScanScratch scan;

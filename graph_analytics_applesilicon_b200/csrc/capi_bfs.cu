@@ -9,6 +9,7 @@
 
 #include "bfs.hpp"
 #include "capi_util.hpp"
+#include "graph_prep.cuh"
 #include "graph_host.hpp"
 
 using namespace gb;
@@ -232,6 +233,14 @@ int gb_bfs_create(const uint32_t* row_ptr, const uint32_t* col_idx, uint64_t n, 
         h->hstage.ensure(16);
         GB_CUDA(cudaStreamSynchronize(h->stream.s));
         *out = h.release();
+    });
+}
+
+int gb_bfs_hub_first(gb_bfs* h) {
+    return guard([&] {
+        GB_REQUIRE(h, "null handle");
+        hubFirstAdjacency(h->rowPtr.get(), h->colIdx.get(), h->n, h->m, h->stream.s);
+        h->hubFirst = true;
     });
 }
 

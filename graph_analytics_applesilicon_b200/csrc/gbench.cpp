@@ -10,6 +10,7 @@
 // GPU variants call the B200 library through include/graph_b200.hpp.  New:
 // gpu_do_persistent (and hybrid, which maps to it), --selector rule|learned,
 // --batch 64 (sources in batches of up to 64 per launch), --block, --hub-min, --grid-blocks, --sel-margin,
+// --hub-first (adjacency lists re-sorted hub-first on the device),
 // gpu_pull_f64, gpu_pull_blocked, and the benchmark graphs synth:rmat22, synth:road1400,
 // synth:web875k, synth:chunglu3m.  Graph preparation (symmetrize, transpose,
 // permute, source picking) runs on the GPU; --host-prep keeps it on the host.
@@ -476,6 +477,7 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
     std::unique_ptr<gpu::GpuBfs> gbfs;
     if (gpuVariant) {
         gbfs = std::make_unique<gpu::GpuBfs>(g.c.row_ptr, g.c.col_idx, g.n(), g.m());
+        if (args.has("hub-first")) gbfs->hubFirst();
         if (o.selector == GB_SELECT_LEARNED) {
             std::string p = args.get("selector-params", exeDir() + "/../selector_single.bin");
             gbfs->setSelector(0, loadSelector(p));

@@ -29,4 +29,8 @@ void uploadCheckedCsr(const gb_csr* g, DevBuf<uint32_t>& rp, DevBuf<uint32_t>& c
 // vertex of v's component.
 void connectedComponents(const uint32_t* rp, const uint32_t* ci, uint64_t n, uint32_t* parent, cudaStream_t st);
 
+// Re-sorts every adjacency list of a device CSR (in place) by descending
+// neighbour degree, ties by id; row_ptr is unchanged.
+void hubFirstAdjacency(const uint32_t* rp, uint32_t* ci, uint64_t n, uint64_t m, cudaStream_t st);
+
 }  // namespace gb

@@ -25,6 +25,8 @@
 // the visit order; a final stable sort of the visit order by component rank
 // gives the concatenation of the components' orders, which is reversed into
 // perm.
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -542,12 +544,75 @@ void rcmOrder(const gb_csr* g, uint32_t* permHost) {
     GB_CUDA(cudaStreamSynchronize(st.s));
 }
 
+// key[i] = (row << b) | rank[ci[i]] for every entry (a warp per row).
+__global__ void rowRankKeysKernel(const uint32_t* rp, const uint32_t* ci, uint64_t n, int b, const uint32_t* rank,
+                                  unsigned long long* keys) {
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw)
+        for (uint32_t i = rp[v] + lane; i < rp[v + 1]; i += 32) keys[i] = (v << b) | rank[ci[i]];
+}
+
+__global__ void rowRankDecodeKernel(const unsigned long long* keys, uint64_t m, int b, const uint32_t* order,
+                                    uint32_t* ci) {
+    const unsigned long long mask = (1ull << b) - 1ull;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+        ci[i] = order[(uint32_t)(keys[i] & mask)];
+}
+
 }  // namespace
+
+void hubFirstAdjacency(const uint32_t* rp, uint32_t* ci, uint64_t n, uint64_t m, cudaStream_t st) {
+    if (m < 2) return;
+    const int b = keyBits(n);
+    ScanScratch sc;
+    DevBuf<uint32_t> order, rank, counts;
+    DevBuf<unsigned long long> keys, tmp;
+    order.ensure(n);
+    rank.ensure(n);
+    keys.ensure(std::max<uint64_t>(n, m));
+    degreeKeysKernel<<<prepGrid(n, 256), 256, 0, st>>>(rp, n, b, true, keys.get());
+    GB_LAUNCH_CHECK();
+    radixSortKeys(keys, tmp, n, 32 + b, sc, st, &counts);
+    keysToOrderKernel<<<prepGrid(n, 256), 256, 0, st>>>(keys.get(), n, b, order.get(), rank.get(), nullptr);
+    GB_LAUNCH_CHECK();
+    rowRankKeysKernel<<<prepGrid(n * 32, 256), 256, 0, st>>>(rp, ci, n, b, rank.get(), keys.get());
+    GB_LAUNCH_CHECK();
+    radixSortKeys(keys, tmp, m, 2 * b, sc, st, &counts);
+    rowRankDecodeKernel<<<prepGrid(m, 256), 256, 0, st>>>(keys.get(), m, b, order.get(), ci);
+    GB_LAUNCH_CHECK();
+    GB_CUDA(cudaStreamSynchronize(st));
+}
+
 }  // namespace gb
 
 using namespace gb;
 
 extern "C" {
+
+int gb_csr_hub_first_gpu(const gb_csr* g, gb_csr* out) {
+    return guard([&] {
+        GB_REQUIRE(g && out, "null argument");
+        Stream st;
+        DevBuf<uint32_t> rp, ci;
+        uploadCheckedCsr(g, rp, ci, st.s);
+        hubFirstAdjacency(rp.get(), ci.get(), g->n, g->m, st.s);
+        uint32_t* hrp = static_cast<uint32_t*>(std::malloc((g->n + 1) * 4));
+        uint32_t* hci = static_cast<uint32_t*>(std::malloc(std::max<uint64_t>(g->m, 1) * 4));
+        if (!hrp || !hci) {
+            std::free(hrp);
+            std::free(hci);
+            throw Error(GB_ERR_OOM, "host allocation failed");
+        }
+        std::memcpy(hrp, g->row_ptr, (g->n + 1) * 4);
+        if (g->m) GB_CUDA(cudaMemcpy(hci, ci.get(), g->m * 4, cudaMemcpyDeviceToHost));
+        out->n = g->n;
+        out->m = g->m;
+        out->flags = g->flags & ~2u;  // rows are no longer sorted by id
+        out->row_ptr = hrp;
+        out->col_idx = hci;
+    });
+}
 
 int gb_reorder_gpu(const gb_csr* g, const char* ordering, uint64_t seed, uint32_t* perm) {
     return guard([&] {

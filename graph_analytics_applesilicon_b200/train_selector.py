@@ -18,6 +18,9 @@ train: the MLP (8 features -> 32 -> 32 -> 5 predicted log2 us) is fitted with
 the library's GPU training kernels (gb_mlp_train, Adam) and written to
 selector_single.npy beside this file, where GpuBfs users and bench.py find it.
 evaluate: learned vs rule persistent BFS on held-out graphs (same depths).
+
+Every handle uses the hub-first adjacency layout (GpuBfs.hub_first), the one
+bench.py and gbench --hub-first run with; --natural keeps the caller's order.
 """
 from __future__ import annotations
 
@@ -30,6 +33,15 @@ import numpy as np
 PKG = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(PKG))
 import graph_analytics_applesilicon_b200 as G  # noqa: E402
+
+
+HUB_FIRST = "--natural" not in sys.argv
+
+
+def handle(g):
+    """A BFS handle with the layout the selector is trained for."""
+    bfs = G.GpuBfs(g)
+    return bfs.hub_first() if HUB_FIRST else bfs
 
 
 def training_graphs():
@@ -63,7 +75,7 @@ def generate_batch(path, batches_per_graph=2, repeats=2, max_rows_per_batch=400)
     feats, times, tags = [], [], []
     for name, g in training_graphs():
         t0 = time.time()
-        bfs = G.GpuBfs(g)
+        bfs = handle(g)
         for b in range(batches_per_graph):
             srcs = G.pick_sources(g, 64, 11 + b)
             f, t = bfs.profile_batch_levels(srcs, repeats=repeats)
@@ -87,7 +99,7 @@ def generate(path, sources_per_graph=3, repeats=3, max_rows_per_source=400):
     feats, times, tags = [], [], []
     for name, g in training_graphs():
         t0 = time.time()
-        bfs = G.GpuBfs(g)
+        bfs = handle(g)
         for s in G.pick_sources(g, sources_per_graph, 7):
             f, t = bfs.profile_levels(int(s), repeats=repeats)
             if len(f) > max_rows_per_source:  # long-diameter graphs: keep an even sample of levels
@@ -147,7 +159,7 @@ def evaluate(params_path=None, sources=8):
     p = np.load(params_path) if params_path else G.default_selector_params("single")
     rows = []
     for name, g in heldout_graphs():
-        bfs = G.GpuBfs(g)
+        bfs = handle(g)
         bfs.set_selector(p, 0)
         srcs = G.pick_sources(g, sources, 3)
         tt = {}
@@ -170,7 +182,7 @@ def evaluate_batch(params_path=None, batches=2):
     p = np.load(params_path) if params_path else G.default_selector_params("batch")
     rows = []
     for name, g in heldout_graphs():
-        bfs = G.GpuBfs(g)
+        bfs = handle(g)
         bfs.set_selector(p, 1)
         tt = {}
         for sel in ("rule", "learned"):
@@ -189,6 +201,7 @@ def evaluate_batch(params_path=None, batches=2):
 
 
 if __name__ == "__main__":
+    sys.argv = [a for a in sys.argv if a != "--natural"]
     cmd = sys.argv[1] if len(sys.argv) > 1 else "evaluate"
     if cmd == "generate":
         generate(sys.argv[2])

@@ -125,6 +125,10 @@ int gb_reorder_gpu(const gb_csr* sym, const char* ordering, uint64_t seed, uint3
 /* reorder::locality (src/graph/reorder.cpp:111-125): mean |u - v| over the
  * stored entries and the fraction with u / 64 == v / 64. */
 int gb_locality(const gb_csr* g, double* mean_gap, double* same_block64);
+/* The hub-first adjacency layout of gb_bfs_hub_first applied to a host CSR on
+ * the GPU: every list sorted by descending neighbour degree, ties by id
+ * (docs/REPORT.md:743-744).  out->flags drops GB_FLAG_SORTED. */
+int gb_csr_hub_first_gpu(const gb_csr* g, gb_csr* out);
 
 /* Generators: src/graph/generators.cpp:8-75 (same graphs, byte for byte). */
 int gb_gen_path(uint32_t n, gb_csr* out);
@@ -234,6 +238,13 @@ uint32_t gb_bfs_last_levels(const gb_bfs* h);
 const uint32_t* gb_bfs_device_dist(const gb_bfs* h);
 /* The CUDA stream the handle launches on (cudaStream_t as void*). */
 void* gb_bfs_stream(const gb_bfs* h);
+/* Hub-first adjacency (the reference's proposed "hub-first neighbor order
+ * inside adjacency lists", docs/REPORT.md:386-398 and 743-744): re-sorts the
+ * handle's device copy of every adjacency list by descending neighbour degree,
+ * ties by id.  Depths are unchanged; bottom-up levels find a frontier parent
+ * sooner, so the "edges" of bottom-up trace records count fewer entries than
+ * in the caller's order.  Stays in effect for the handle's lifetime. */
+int gb_bfs_hub_first(gb_bfs* h);
 
 /* Learned selector: load MLP parameters (layout of gb_selector_param_count) for
  * single-source (which = 0) or batched (which = 1) persistent runs. */

@@ -73,6 +73,8 @@ public:
     void setSelector(int which, const std::vector<float>& params) {
         check(gb_bfs_set_selector(h_, which, params.data(), params.size()));
     }
+    // Hub-first adjacency order on the device (same depths, earlier bottom-up exits).
+    void hubFirst() { check(gb_bfs_hub_first(h_)); }
     double lastGpuMs() const { return gb_bfs_last_gpu_ms(h_); }
     uint32_t lastLevels() const { return gb_bfs_last_levels(h_); }
     // Device pointer of the last result (GpuBfs::dist() for device-side callers).

@@ -62,3 +62,36 @@ def test_gpu_orderings_errors(gb):
     g = gb.gen.path(10)
     assert np.array_equal(gb.reorder_gpu(g, "random", 4), gb.random_perm(10, 4))
     assert np.array_equal(gb.reorder_gpu(g, "original"), np.arange(10, dtype=np.uint32))
+
+
+def _hub_first_numpy(g):
+    deg = np.diff(g.row_ptr.astype(np.int64))
+    rows = np.repeat(np.arange(g.n, dtype=np.int64), deg)
+    col = g.col_idx.astype(np.int64)
+    return g.col_idx[np.lexsort((col, -deg[col], rows))]
+
+
+@pytest.mark.parametrize("case", ["rmat16", "chunglu", "star", "road"])
+def test_hub_first_layout_and_bfs(gb, oracle, case):
+    """gb_csr_hub_first_gpu equals a numpy lexsort; a BFS handle with the
+    hub-first layout returns the oracle's depths, and with the alpha/beta rule
+    the oracle's per-level directions, frontier sizes and top-down edges."""
+    g = {"rmat16": lambda: gb.gen.rmat(16, 16, False, 5), "chunglu": lambda: gb.gen.chung_lu(100000, 2.2, 20.0, 6),
+         "star": lambda: gb.gen.star(5000), "road": lambda: gb.gen.road(120, 120, 0.04, 0.005, 7)}[case]()
+    h = gb.hub_first_gpu(g)
+    assert np.array_equal(h.row_ptr, g.row_ptr) and np.array_equal(h.col_idx, _hub_first_numpy(g))
+    og = _as_oracle(oracle, g)
+    bfs = gb.GpuBfs(g).hub_first()
+    srcs = gb.pick_sources(g, 8, 3)
+    rule = gb.BfsOptions(selector="rule")
+    for s in srcs:
+        want = oracle.bfs_serial(og, int(s))
+        for variant in ("gpu_do", "gpu_do_persistent"):
+            assert np.array_equal(bfs.run(variant, int(s), opts=rule), want), (case, variant, s)
+        d, tr = bfs.run("gpu_do_persistent", int(s), opts=rule, trace=True)
+        _, otr = oracle.bfs_do(og, int(s))
+        assert [(t["direction"], t["frontier"]) for t in tr] == [(o[1], o[2]) for o in otr]
+        assert [t["edges"] for t in tr if t["direction"] == "T"] == [o[3] for o in otr if o[1] == "T"]
+    batch = bfs.run_batch(srcs)
+    for i, s in enumerate(srcs):
+        assert np.array_equal(batch[i], oracle.bfs_serial(og, int(s)))
