@@ -15,7 +15,8 @@ source's component / time (src/bench/main.cpp:329-370).
   value       device-resident: graph in HBM, dist kept on the device, CUDA
               events on the library's stream around the 64 launches.
   e2e         the same call with a pinned host output buffer per source: the
-              16.8 MB depth array comes back to the host inside the timed region.
+              16.8 MB uint32 depth array comes back to the host inside the timed
+              region (over PCIe as 1 byte per depth, widened on the host).
   roofline    persistent kernel, HBM bound: graph-pass bytes 4(n+1)+4m+4n per
               traversal / mean launch time, against the measured copy peak.
   cpu_baseline the reference's own cpu_do (oracle/_ref, all host cores) on a
@@ -125,6 +126,16 @@ def build_graph(G, scale=SCALE, nsrc=NSRC, gpu_prep=True):
     srcs = G.pick_sources_gpu(g, nsrc, 1) if gpu_prep else G.pick_sources(g, nsrc, 1)
     log(f"graph n={g.n} m={g.m} built in {time.time() - t:.1f}s")
     return g, srcs
+
+
+def depth_wire_bytes(n, levels):
+    """Bytes per depth on the PCIe wire: the library packs depths to 1 or 2
+    bytes when the level count allows (arrays of 2^18 vertices or more)."""
+    if n >= (1 << 18) and levels < 255:
+        return 1
+    if n >= (1 << 18) and levels < 65535:
+        return 2
+    return 4
 
 
 def component_edges(g, dist):
@@ -295,6 +306,7 @@ def bfs_config_workload(args, world, rank, local):
     ob = min(batch_cands.values(), key=lambda x: x[0])[1]
     # exactness of the batch against single-source runs (size-independent)
     d64 = bfs.run_batch(srcs64, opts=ob)
+    batch_levels = bfs.lastLevels()
     for i in (0, 17, 63):
         assert np.array_equal(d64[i], bfs.run("gpu_do_persistent", int(srcs64[i]))), "batch != single"
     valid = check_depths(g, d64[0], int(srcs64[0]))
@@ -341,7 +353,8 @@ def bfs_config_workload(args, world, rank, local):
                        "single_tuned": {"block": o1.block, "grid_blocks": o1.grid_blocks, "hub_min": o1.hub_min},
                        "parallelism": f"replicas{world}"},
             "e2e": {"value": world * e64 / (e2e * 1e-3) / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 256,
-                    "d2h_bytes_per_step": 4 * 64 * g.n},
+                    "d2h_bytes_per_step": depth_wire_bytes(g.n, batch_levels) * 64 * g.n,
+                    "result_bytes_per_step": 4 * 64 * g.n},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_source": peak_kind, "kernel": "batchBfsKernel",
@@ -652,8 +665,10 @@ def main():
     # exactness of one result (size-independent check) and TEPS denominators
     comp = []
     d0 = None
+    max_levels = 0
     for i, s in enumerate(srcs):
         d = bfs.run("gpu_do_persistent", int(s), opts=opts)
+        max_levels = max(max_levels, bfs.lastLevels())
         comp.append(component_edges(g, d))
         if i == 0:
             d0 = d.copy()
@@ -750,7 +765,8 @@ def main():
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (CSR 293 MB)",
                    "edges_per_step": edges_per_step},
         "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),
-                "d2h_bytes_per_step": 4 * g.n * len(srcs)},
+                "d2h_bytes_per_step": depth_wire_bytes(g.n, max_levels) * g.n * len(srcs),
+                "result_bytes_per_step": 4 * g.n * len(srcs)},
         "gpu_launches": len(srcs) * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,

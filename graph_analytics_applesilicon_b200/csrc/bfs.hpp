@@ -29,6 +29,13 @@ struct GbPCounters {
     unsigned long long pad[2];
 };
 
+struct gb_bfs;
+namespace gb {
+// Copies count depths from device d to host out (uint32, unreached ~0), packed
+// to 1 or 2 bytes per depth over PCIe when `levels` allows (depth_out.cu).
+void copyDepthsToHost(gb_bfs* h, const uint32_t* d, uint64_t count, uint32_t* out, uint32_t levels);
+}  // namespace gb
+
 struct gb_bfs {
     uint64_t n = 0, m = 0;
     std::vector<uint32_t> hostRowPtr;  // degrees of sources on the host
@@ -66,6 +73,16 @@ struct gb_bfs {
     // learned selector parameters (single-source, batched)
     gb::DevBuf<float> selParams[2];
     bool selLoaded[2] = {false, false};
+
+    // packed depth transfer to the host (depth_out.cu)
+    gb::DevBuf<uint8_t> packDev;
+    gb::HostPinned<uint8_t> packHost;
+    gb::DevBuf<unsigned> packFlag;
+    gb::HostPinned<unsigned> packFlagHost;
+    std::vector<cudaEvent_t> packEv;
+    ~gb_bfs() {
+        for (cudaEvent_t e : packEv) cudaEventDestroy(e);
+    }
 
     double lastGpuMs = 0;
     uint32_t lastLevels = 0;

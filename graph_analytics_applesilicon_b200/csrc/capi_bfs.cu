@@ -273,10 +273,7 @@ int gb_bfs_run(gb_bfs* h, int variant, uint32_t source, uint32_t* out_host, cons
             case GB_BFS_PERSISTENT: h->runPersistent(source, o, tp); break;
             default: throw Error(GB_ERR_ARG, "unknown BFS variant " + std::to_string(variant));
         }
-        if (out_host) {
-            GB_CUDA(cudaMemcpyAsync(out_host, h->dist.get(), h->n * 4, cudaMemcpyDeviceToHost, h->stream.s));
-            GB_CUDA(cudaStreamSynchronize(h->stream.s));
-        }
+        if (out_host) copyDepthsToHost(h, h->dist.get(), h->n, out_host, h->lastLevels);
         if (nlev) *nlev = tr.size();
         if (trace) {
             std::memcpy(trace, tr.data(), std::min(cap, tr.size()) * sizeof(gb_level));

@@ -57,11 +57,7 @@ int gb_bfs_run_batch(gb_bfs* h, const uint32_t* sources, int k, uint32_t* out_ho
         gb_bfs_options o = optsOrDefault(opt);
         std::vector<gb_level> tr;
         h->runBatch(sources, k, o, (trace || nlev) ? &tr : nullptr);
-        if (out_host) {
-            GB_CUDA(cudaMemcpyAsync(out_host, h->bDist.get(), (uint64_t)k * h->n * 4, cudaMemcpyDeviceToHost,
-                                    h->stream.s));
-            GB_CUDA(cudaStreamSynchronize(h->stream.s));
-        }
+        if (out_host) copyDepthsToHost(h, h->bDist.get(), (uint64_t)k * h->n, out_host, h->lastLevels);
         if (nlev) *nlev = tr.size();
         if (trace) {
             std::memcpy(trace, tr.data(), std::min(cap, tr.size()) * sizeof(gb_level));

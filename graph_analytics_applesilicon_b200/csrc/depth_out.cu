@@ -1,0 +1,92 @@
+// depth_out.cu -- returning BFS depths to host memory.  A depth array is
+// 4 bytes per vertex, but a traversal of L levels only needs depths below L:
+// when L < 255 (or < 65535) the depths travel over PCIe as 1 (or 2) bytes per
+// vertex, sentinel ~0 for unreached, in chunks whose host-side widening to
+// uint32 (OpenMP threads) overlaps the copy of the next chunk.  The pack
+// kernel also checks every depth against the width, so a wrong level count
+// can only cost a plain copy, never a wrong result.
+#include <omp.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "bfs.hpp"
+
+namespace gb {
+namespace {
+
+constexpr uint64_t kPackMin = 1u << 18;   // smaller arrays go as one plain copy
+constexpr uint64_t kPackChunk = 1u << 20;  // vertices per pipelined chunk
+
+template <typename T>
+__global__ void packDepthsKernel(const uint32_t* d, uint64_t count, T* out, unsigned* overflow) {
+    const uint32_t sentinel = (uint32_t)(T)~0u;
+    bool bad = false;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = d[i];
+        bad |= v != 0xFFFFFFFFu && v >= sentinel;
+        out[i] = v == 0xFFFFFFFFu ? (T)sentinel : (T)v;
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(overflow, 1u);
+}
+
+template <typename T>
+void widen(const T* in, uint32_t* out, uint64_t count) {
+    const uint32_t sentinel = (uint32_t)(T)~0u;
+    const int threads = std::max(1, std::min(16, omp_get_max_threads()));
+#pragma omp parallel for num_threads(threads) schedule(static) if (count >= (1u << 16))
+    for (int64_t i = 0; i < (int64_t)count; ++i) {
+        const uint32_t v = in[i];
+        out[i] = v == sentinel ? 0xFFFFFFFFu : v;
+    }
+}
+
+template <typename T>
+bool packedCopy(gb_bfs* h, const uint32_t* d, uint64_t count, uint32_t* out) {
+    cudaStream_t st = h->stream.s;
+    h->packDev.ensure(count * sizeof(T));
+    h->packHost.ensure(count * sizeof(T));
+    h->packFlag.ensure(1);
+    h->packFlagHost.ensure(1);
+    GB_CUDA(cudaMemsetAsync(h->packFlag.get(), 0, 4, st));
+    T* dp = reinterpret_cast<T*>(h->packDev.get());
+    T* hp = reinterpret_cast<T*>(h->packHost.p);
+    packDepthsKernel<T><<<deviceSmCount() * 8, 256, 0, st>>>(d, count, dp, h->packFlag.get());
+    GB_LAUNCH_CHECK();
+    const uint64_t chunks = (count + kPackChunk - 1) / kPackChunk;
+    while (h->packEv.size() < chunks) {
+        cudaEvent_t e;
+        GB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        h->packEv.push_back(e);
+    }
+    for (uint64_t c = 0; c < chunks; ++c) {
+        const uint64_t lo = c * kPackChunk, len = std::min(kPackChunk, count - lo);
+        GB_CUDA(cudaMemcpyAsync(hp + lo, dp + lo, len * sizeof(T), cudaMemcpyDeviceToHost, st));
+        if (c + 1 == chunks)
+            GB_CUDA(cudaMemcpyAsync(h->packFlagHost.p, h->packFlag.get(), 4, cudaMemcpyDeviceToHost, st));
+        GB_CUDA(cudaEventRecord(h->packEv[c], st));
+    }
+    for (uint64_t c = 0; c < chunks; ++c) {
+        const uint64_t lo = c * kPackChunk, len = std::min(kPackChunk, count - lo);
+        GB_CUDA(cudaEventSynchronize(h->packEv[c]));
+        widen(hp + lo, out + lo, len);
+    }
+    return *h->packFlagHost.p == 0;
+}
+
+}  // namespace
+
+void copyDepthsToHost(gb_bfs* h, const uint32_t* d, uint64_t count, uint32_t* out, uint32_t levels) {
+    bool done = false;
+    if (count >= kPackMin) {
+        if (levels < 255) done = packedCopy<uint8_t>(h, d, count, out);
+        else if (levels < 65535) done = packedCopy<uint16_t>(h, d, count, out);
+    }
+    if (!done) {
+        GB_CUDA(cudaMemcpyAsync(out, d, count * 4, cudaMemcpyDeviceToHost, h->stream.s));
+        GB_CUDA(cudaStreamSynchronize(h->stream.s));
+    }
+}
+
+}  // namespace gb
