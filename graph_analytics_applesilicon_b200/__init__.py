@@ -119,6 +119,8 @@ def lib():
             "gb_csr_free": (None, [P]),
             "gb_csr_load": (C.c_int, [C.c_char_p, P]),
             "gb_csr_save": (C.c_int, [P, C.c_char_p]),
+            "gb_csr_load_pinned": (C.c_int, [C.c_char_p, P]),
+            "gb_bfs_create_from_file": (C.c_int, [C.c_char_p, vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
             "gb_csr_validate": (C.c_int, [P, C.c_char_p, C.c_size_t]),
             "gb_csr_from_edges": (C.c_int, [C.c_uint64, _u32p, _u32p, C.c_uint64, C.c_int, P]),
             "gb_csr_transpose": (C.c_int, [P, P]),
@@ -392,6 +394,12 @@ def load(path: str) -> Graph:
     return _make(lib().gb_csr_load, path.encode())
 
 
+def load_pinned(path: str) -> Graph:
+    """graph::load into page-locked memory (returned here as numpy copies; C
+    callers keep the pinned arrays and upload them at full PCIe speed)."""
+    return _make(lib().gb_csr_load_pinned, path.encode())
+
+
 def save(g: Graph, path: str) -> None:
     check(lib().gb_csr_save(C.byref(g._c()), path.encode()))
 
@@ -427,6 +435,17 @@ def _levels(buf, k):
 
 class GpuBfs:
     """gpu::GpuBfs (src/metal/bfs_gpu.hpp:35-105): one upload of a symmetric CSR."""
+
+    @classmethod
+    def from_file(cls, path: str) -> "GpuBfs":
+        """A handle whose graph streams from a symmetric .bin file straight
+        into GPU memory (gb_bfs_create_from_file)."""
+        self = cls.__new__(cls)
+        self._h = C.c_void_p()
+        n, m = C.c_uint64(0), C.c_uint64(0)
+        check(lib().gb_bfs_create_from_file(os.fsencode(path), C.byref(self._h), C.byref(n), C.byref(m)))
+        self.n, self.m = n.value, m.value
+        return self
 
     def __init__(self, g: Graph):
         self.n, self.m = g.n, g.m

@@ -89,17 +89,10 @@ int gb_device_info(char* name, size_t cap, int* sm_count, int* cc_major, int* cc
 
 void gb_csr_free(gb_csr* g) {
     if (!g) return;
-    std::free(g->row_ptr);
-    std::free(g->col_idx);
+    if (!freePinnedArray(g->row_ptr)) std::free(g->row_ptr);
+    if (!freePinnedArray(g->col_idx)) std::free(g->col_idx);
     g->row_ptr = g->col_idx = nullptr;
     g->n = g->m = 0;
-}
-
-int gb_csr_load(const char* path, gb_csr* out) {
-    return guard([&] {
-        GB_REQUIRE(path, "null path");
-        toC(csrLoad(path), out);
-    });
 }
 
 int gb_csr_save(const gb_csr* g, const char* path) {
@@ -228,6 +221,7 @@ int gb_bfs_create(const uint32_t* row_ptr, const uint32_t* col_idx, uint64_t n, 
         h->dist.ensure(n + 4);
         GB_CUDA(cudaMemcpyAsync(h->rowPtr.get(), row_ptr, (n + 1) * 4, cudaMemcpyHostToDevice, h->stream.s));
         if (m) GB_CUDA(cudaMemcpyAsync(h->colIdx.get(), col_idx, m * 4, cudaMemcpyHostToDevice, h->stream.s));
+        checkDeviceCsr(h->rowPtr.get(), h->colIdx.get(), n, m, h->stream.s);  // ids below n before any traversal
         h->stats.ensure(1);
         h->hstats.ensure(1);
         h->hstage.ensure(16);

@@ -3,6 +3,7 @@
 #include <memory>
 
 #include "capi_util.hpp"
+#include "graph_prep.cuh"
 #include "pagerank.hpp"
 
 using namespace gb;
@@ -41,6 +42,7 @@ int gb_pr_create(uint64_t n, const uint32_t* out_row_ptr, const uint32_t* out_co
             h->colOut.ensure(out_m + 4);
             GB_CUDA(cudaMemcpy(h->rowOut.get(), out_row_ptr, (n + 1) * 4, cudaMemcpyHostToDevice));
             if (out_m) GB_CUDA(cudaMemcpy(h->colOut.get(), out_col_idx, out_m * 4, cudaMemcpyHostToDevice));
+            checkDeviceCsr(h->rowOut.get(), h->colOut.get(), n, out_m, 0);
         }
         if (in_row_ptr) {
             GB_REQUIRE(in_m == 0 || in_col_idx, "null in col_idx");
@@ -52,6 +54,7 @@ int gb_pr_create(uint64_t n, const uint32_t* out_row_ptr, const uint32_t* out_co
             GB_CUDA(cudaMemset(h->colIn.get(), 0, (in_m + 4) * 4));
             GB_CUDA(cudaMemcpy(h->rowIn.get(), in_row_ptr, (n + 1) * 4, cudaMemcpyHostToDevice));
             if (in_m) GB_CUDA(cudaMemcpy(h->colIn.get(), in_col_idx, in_m * 4, cudaMemcpyHostToDevice));
+            checkDeviceCsr(h->rowIn.get(), h->colIn.get(), n, in_m, 0);
             h->hostRowIn.assign(in_row_ptr, in_row_ptr + n + 1);
             h->hostColIn.assign(in_col_idx, in_col_idx + in_m);
         }

@@ -12,6 +12,8 @@ extern thread_local std::string g_lastError;
 int guardStatus(const std::exception_ptr& ep);
 void toC(HostCsr&& g, gb_csr* out);
 HostCsr fromC(const gb_csr* g);
+// Releases an array of gb_csr_load_pinned (page-locked); false for any other pointer.
+bool freePinnedArray(void* p);
 
 template <class F>
 int guard(F&& f) {

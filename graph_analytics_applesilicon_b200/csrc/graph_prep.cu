@@ -363,6 +363,15 @@ void uploadCsr(const gb_csr* g, DevBuf<uint32_t>& rp, DevBuf<uint32_t>& ci, cuda
 
 }  // namespace
 
+void checkDeviceCsr(const uint32_t* rp, const uint32_t* ci, uint64_t n, uint64_t m, cudaStream_t st) {
+    DevBuf<unsigned> bad;
+    bad.ensure(1);
+    GB_CUDA(cudaMemsetAsync(bad.get(), 0, 4, st));
+    checkCsrKernel<<<prepGrid(std::max(n, m), 256), 256, 0, st>>>(rp, ci, n, m, bad.get());
+    GB_LAUNCH_CHECK();
+    requireChecks(bad, st);
+}
+
 void uploadCheckedCsr(const gb_csr* g, DevBuf<uint32_t>& rp, DevBuf<uint32_t>& ci, cudaStream_t st) {
     GB_REQUIRE(g && g->row_ptr && (g->m == 0 || g->col_idx), "null CSR arrays");
     GB_REQUIRE(g->n >= 1 && g->n < 0xFFFFFFFFull, "graph prep: n must be in [1, 2^32 - 1)");

@@ -25,6 +25,9 @@ void keysToCsr(DevBuf<unsigned long long>& keys, uint64_t N, uint64_t n, int b, 
 // Uploads a host CSR and checks it on the device (row_ptr from 0 to m and
 // non-decreasing, every column below n); throws GB_ERR_ARG otherwise.
 void uploadCheckedCsr(const gb_csr* g, DevBuf<uint32_t>& rp, DevBuf<uint32_t>& ci, cudaStream_t st);
+// Checks a device CSR (row_ptr non-decreasing, every column below n); throws
+// GB_ERR_ARG otherwise.
+void checkDeviceCsr(const uint32_t* rp, const uint32_t* ci, uint64_t n, uint64_t m, cudaStream_t st);
 // Connected components of a symmetric device CSR: parent[v] = the smallest
 // vertex of v's component.
 void connectedComponents(const uint32_t* rp, const uint32_t* ci, uint64_t n, uint32_t* parent, cudaStream_t st);

@@ -58,6 +58,12 @@ void gb_csr_free(gb_csr* g);
 /* graph::load / graph::save, "GGPUCSR1" format (src/graph/csr.cpp:30-84). */
 int gb_csr_load(const char* path, gb_csr* out);
 int gb_csr_save(const gb_csr* g, const char* path);
+/* graph::load for a discrete GPU (src/graph/csr.cpp:54-84 maps the file and
+ * lets the GPU read it in place; here it has to cross PCIe): the same checks
+ * and result as gb_csr_load, with both arrays in page-locked host memory read
+ * by several threads, so every later upload runs at full PCIe speed.
+ * gb_csr_free releases them. */
+int gb_csr_load_pinned(const char* path, gb_csr* out);
 /* graph::validate (src/graph/csr.cpp:86-104); msg gets "" when valid. */
 int gb_csr_validate(const gb_csr* g, char* msg, size_t cap);
 /* graph::fromEdgeList (src/graph/csr.cpp:146-163). */
@@ -219,6 +225,13 @@ typedef struct gb_bfs gb_bfs;
 int gb_bfs_create(const uint32_t* row_ptr, const uint32_t* col_idx, uint64_t n, uint64_t m,
                   gb_bfs** out);
 int gb_bfs_destroy(gb_bfs* h);
+/* GpuBfs from a symmetric .bin file (graph::load + GpuBfs(ctx, g),
+ * src/graph/csr.cpp:54-84, src/metal/bfs_gpu.hpp:37): the adjacency streams
+ * from the file into the handle's device memory through two pinned staging
+ * buffers, read and copy overlapped, with no host copy of the whole graph.
+ * A directed file is rejected (GB_ERR_ARG): BFS runs on the symmetric graph.
+ * n_out / m_out (may be null) receive the graph's sizes. */
+int gb_bfs_create_from_file(const char* path, gb_bfs** out, uint64_t* n_out, uint64_t* m_out);
 /* GpuBfs::run* (src/metal/bfs_gpu.hpp:43-66).  out_host: n entries written on
  * return, or NULL to leave the result in device memory (gb_bfs_device_dist).
  * trace: optional per-level records (cap entries, *nlev = levels run). */

@@ -34,6 +34,8 @@ public:
     GpuBfs(const uint32_t* row_ptr, const uint32_t* col_idx, uint64_t n, uint64_t m) : n_(n) {
         check(gb_bfs_create(row_ptr, col_idx, n, m, &h_));
     }
+    // From a symmetric .bin file, streamed straight into GPU memory.
+    explicit GpuBfs(const char* path) : n_(0) { check(gb_bfs_create_from_file(path, &h_, &n_, nullptr)); }
     ~GpuBfs() { gb_bfs_destroy(h_); }
     GpuBfs(const GpuBfs&) = delete;
     GpuBfs& operator=(const GpuBfs&) = delete;
