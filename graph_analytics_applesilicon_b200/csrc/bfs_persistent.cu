@@ -242,69 +242,94 @@ __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e
 // for the first neighbour in the frontier bitmap (early exit).  The found
 // lanes form the next frontier word (__ballot_sync); the owning warp writes
 // it and the visited word with plain stores.
+// The rest of one vertex's bottom-up scan after its first entry missed: the
+// first parent in the frontier, scanning in list order from i; aligned groups
+// of 4 entries are loaded at once and their 4 frontier words fetched
+// together, so a step costs two dependent loads for 4 entries.  Returns one
+// past the first hit, or e when there is none (found tells which).
+__device__ __forceinline__ uint32_t buScanFrom(const PArgs& a, const uint32_t* front, uint32_t i, uint32_t e,
+                                               bool& found) {
+    for (; i < e && (i & 3u); ++i) {
+        const uint32_t u = a.col_idx[i];
+        if ((front[u >> 5] >> (u & 31)) & 1u) {
+            found = true;
+            return i + 1;
+        }
+    }
+    for (; i + 4 <= e; i += 4) {
+        const uint4 q = *reinterpret_cast<const uint4*>(a.col_idx + i);
+        const uint32_t f0 = front[q.x >> 5], f1 = front[q.y >> 5], f2 = front[q.z >> 5], f3 = front[q.w >> 5];
+        const unsigned hits = ((f0 >> (q.x & 31)) & 1u) | (((f1 >> (q.y & 31)) & 1u) << 1) |
+                              (((f2 >> (q.z & 31)) & 1u) << 2) | (((f3 >> (q.w & 31)) & 1u) << 3);
+        if (hits) {
+            found = true;
+            return i + __ffs(hits);
+        }
+    }
+    for (; i < e; ++i) {
+        const uint32_t u = a.col_idx[i];
+        if ((front[u >> 5] >> (u & 31)) & 1u) {
+            found = true;
+            return i + 1;
+        }
+    }
+    return e;
+}
+
+// Bottom-up level: each unvisited vertex looks for its first parent in the
+// frontier bitmap.  A warp takes kBuWords bitmap words (32 vertices each, a
+// lane per vertex) per round and issues their loads stage by stage -- visited
+// words, then row bounds, then first entries, then frontier bits -- so the
+// four dependent loads of the words overlap instead of running one word
+// after another; a vertex whose first entry is not a parent (rare once lists
+// are hub-first) continues with buScanFrom.
+constexpr int kBuWords = 4;
+
 __device__ void buLevel(const PArgs& a, uint32_t level, Acc& acc) {
     const uint32_t* front = a.bm[level % 3];
     uint32_t* next = a.bm[(level + 1) % 3];
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const unsigned lane = laneId();
-    for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < a.words; w += nwarps) {
-        const uint32_t vw = a.visited[w];
-        if (vw == kFull) continue;  // warp-uniform
-        const uint32_t v = (uint32_t)(w * 32 + lane);
-        bool found = false;
-        uint32_t b = 0, e = 0;
-        if (!((vw >> lane) & 1u)) {
-            b = a.row_ptr[v];
-            e = a.row_ptr[v + 1];
-            // First parent in the frontier, scanning in list order; aligned
-            // groups of 4 entries are loaded at once and their 4 frontier
-            // words fetched together, so a step costs two dependent loads
-            // for 4 entries.  `stop` is one past the first hit (or e).
-            uint32_t stop = e;
-            uint32_t i = b;
-            for (; i < e && (i & 3u); ++i) {
-                const uint32_t u = a.col_idx[i];
-                if ((front[u >> 5] >> (u & 31)) & 1u) {
-                    stop = i + 1;
-                    found = true;
-                    break;
-                }
-            }
-            if (!found) {
-                for (; i + 4 <= e; i += 4) {
-                    const uint4 q = *reinterpret_cast<const uint4*>(a.col_idx + i);
-                    const uint32_t f0 = front[q.x >> 5], f1 = front[q.y >> 5], f2 = front[q.z >> 5],
-                                   f3 = front[q.w >> 5];
-                    const unsigned hits = ((f0 >> (q.x & 31)) & 1u) | (((f1 >> (q.y & 31)) & 1u) << 1) |
-                                          (((f2 >> (q.z & 31)) & 1u) << 2) | (((f3 >> (q.w & 31)) & 1u) << 3);
-                    if (hits) {
-                        stop = i + __ffs(hits);
-                        found = true;
-                        break;
-                    }
-                }
-            }
-            if (!found) {
-                for (; i < e; ++i) {
-                    const uint32_t u = a.col_idx[i];
-                    if ((front[u >> 5] >> (u & 31)) & 1u) {
-                        stop = i + 1;
-                        found = true;
-                        break;
-                    }
-                }
-            }
-            acc.exam += stop - b;
+    for (uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w0 < a.words;
+         w0 += nwarps * kBuWords) {
+        uint32_t vw[kBuWords], b[kBuWords], e[kBuWords], u[kBuWords];
+        bool need[kBuWords], found[kBuWords];
+#pragma unroll
+        for (int k = 0; k < kBuWords; ++k) {
+            const uint64_t w = w0 + (uint64_t)k * nwarps;
+            vw[k] = w < a.words ? a.visited[w] : kFull;
+            need[k] = !((vw[k] >> lane) & 1u);
+            found[k] = false;
         }
-        const unsigned F = __ballot_sync(kFull, found);
-        if (found) {
-            a.dist[v] = level + 1;
-            acc.deg += e - b;
-            acc.found++;
+#pragma unroll
+        for (int k = 0; k < kBuWords; ++k) {
+            const uint32_t v = (uint32_t)((w0 + (uint64_t)k * nwarps) * 32 + lane);
+            b[k] = need[k] ? a.row_ptr[v] : 0u;
+            e[k] = need[k] ? a.row_ptr[v + 1] : 0u;
         }
-        if (lane == 0 && F) {
-            next[w] = F;
-            a.visited[w] = vw | F;
+#pragma unroll
+        for (int k = 0; k < kBuWords; ++k) u[k] = b[k] < e[k] ? a.col_idx[b[k]] : 0u;
+#pragma unroll
+        for (int k = 0; k < kBuWords; ++k) {
+            if (b[k] < e[k] && ((front[u[k] >> 5] >> (u[k] & 31)) & 1u)) {
+                found[k] = true;
+                acc.exam += 1;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kBuWords; ++k) {
+            if (need[k] && !found[k]) acc.exam += (b[k] < e[k] ? buScanFrom(a, front, b[k] + 1, e[k], found[k]) : e[k]) - b[k];
+            const unsigned F = __ballot_sync(kFull, found[k]);
+            const uint64_t w = w0 + (uint64_t)k * nwarps;
+            if (found[k]) {
+                a.dist[w * 32 + lane] = level + 1;
+                acc.deg += e[k] - b[k];
+                acc.found++;
+            }
+            if (lane == 0 && F) {
+                next[w] = F;
+                a.visited[w] = vw[k] | F;
+            }
         }
     }
 }
