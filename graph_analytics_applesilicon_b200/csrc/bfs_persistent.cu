@@ -68,20 +68,12 @@ struct Acc {
     unsigned long long found = 0, deg = 0, exam = 0;
 };
 
-// Claim u for level+1 (all 32 lanes call together) and append it to the next
-// frontier: bitmap bit, queue entry (degree < hub_min) or hub entry.
-__device__ __forceinline__ void discover(const PArgs& a, bool has, uint32_t u, uint32_t level, GbPCounters* cur,
-                                         uint32_t* bmNext, uint32_t nq, Acc& acc, bool precheck) {
-    bool claimed = false;
+// Append a claimed u (all 32 lanes call together) to the next frontier:
+// depth, bitmap bit, queue entry (degree < hub_min) or hub entry.
+__device__ __forceinline__ void appendClaimed(const PArgs& a, bool claimed, uint32_t u, uint32_t st, uint32_t en,
+                                              uint32_t level, GbPCounters* cur, uint32_t* bmNext, uint32_t nq,
+                                              Acc& acc) {
     const uint32_t w = u >> 5, bit = 1u << (u & 31);
-    uint32_t st = 0, en = 0;
-    // Small levels claim directly (one dependent round trip less); large ones
-    // read the visited word first to spare atomics on visited neighbours.
-    if (has && (!precheck || !(a.visited[w] & bit))) {
-        st = a.row_ptr[u];  // issued alongside the claim: no extra dependent step
-        en = a.row_ptr[u + 1];
-        claimed = !(atomicOr(&a.visited[w], bit) & bit);
-    }
     if (!__any_sync(kFull, claimed)) return;
     const uint32_t d = claimed ? en - st : 0u;
     if (claimed) {
@@ -107,6 +99,36 @@ __device__ __forceinline__ void discover(const PArgs& a, bool has, uint32_t u, u
         a.hs[nq][i] = st;
         a.ho[nq][i] = old & kHubMask;
     }
+}
+
+// Claim K vertices per lane for level+1 and append the claimed ones (all 32
+// lanes call together).  The K claims are issued stage by stage -- visited
+// words (large levels read them first to spare atomics on visited
+// neighbours), row bounds and atomicOr claims -- so their round trips overlap
+// rather than run one claim after another.
+template <int K>
+__device__ __forceinline__ void discoverN(const PArgs& a, const bool* has, const uint32_t* u, uint32_t level,
+                                          GbPCounters* cur, uint32_t* bmNext, uint32_t nq, Acc& acc, bool precheck) {
+    bool cand[K];
+    uint32_t st[K], en[K], old[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) cand[k] = has[k];
+    if (precheck) {
+        uint32_t vw[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) vw[k] = cand[k] ? a.visited[u[k] >> 5] : 0u;
+#pragma unroll
+        for (int k = 0; k < K; ++k) cand[k] = cand[k] && !(vw[k] & (1u << (u[k] & 31)));
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        st[k] = cand[k] ? a.row_ptr[u[k]] : 0u;
+        en[k] = cand[k] ? a.row_ptr[u[k] + 1] : 0u;
+        old[k] = cand[k] ? atomicOr(&a.visited[u[k] >> 5], 1u << (u[k] & 31)) : ~0u;
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        appendClaimed(a, !(old[k] & (1u << (u[k] & 31))), u[k], st[k], en[k], level, cur, bmNext, nq, acc);
 }
 
 template <int NT>
@@ -177,7 +199,7 @@ __device__ void tdTile(const PArgs& a, Smem<NT>& sm, uint32_t item, uint32_t S, 
             }
         }
 #pragma unroll
-        for (int k = 0; k < EPT; ++k) discover(a, has[k], u[k], level, cur, bmNext, qc ^ 1u, acc, pre);
+        discoverN<EPT>(a, has, u, level, cur, bmNext, qc ^ 1u, acc, pre);
     }
     __syncthreads();
 }
@@ -198,10 +220,11 @@ __device__ __forceinline__ void tdGroups(const PArgs& a, uint32_t S, unsigned G,
         const bool has = idx < S;
         const uint32_t st = has ? a.qs[qc][idx] : 0u, d = has ? a.qd[qc][idx] : 0u;
         const uint32_t maxd = __reduce_max_sync(kFull, d);
-        for (uint32_t e0 = 0; e0 < maxd; e0 += G) {
+        for (uint32_t e0 = 0; e0 < maxd; e0 += 2 * G) {  // two rounds per step: their claims overlap
             const uint32_t e = e0 + (lane & (G - 1));
-            const bool he = e < d;
-            discover(a, he, he ? a.col_idx[st + e] : 0u, level, cur, bmNext, qc ^ 1u, acc, pre);
+            const bool he[2] = {e < d, e + G < d};
+            const uint32_t u[2] = {he[0] ? a.col_idx[st + e] : 0u, he[1] ? a.col_idx[st + e + G] : 0u};
+            discoverN<2>(a, he, u, level, cur, bmNext, qc ^ 1u, acc, pre);
         }
     }
 }
@@ -233,7 +256,7 @@ __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e
             }
         }
 #pragma unroll
-        for (int k = 0; k < 2; ++k) discover(a, has[k], u[k], level, cur, bmNext, qc ^ 1u, acc, pre);
+        discoverN<2>(a, has, u, level, cur, bmNext, qc ^ 1u, acc, pre);
     }
     __syncthreads();
 }
