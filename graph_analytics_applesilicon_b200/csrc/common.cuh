@@ -170,18 +170,24 @@ __device__ __forceinline__ unsigned warpAppend(bool want, unsigned* counter) {
 // other blocks' writes, so thread 0 may read shared counters right away.
 __device__ __forceinline__ bool gridArriveWait(unsigned* bar, unsigned* err, unsigned long long spinLimit,
                                                unsigned nblocks) {
-    unsigned inc = (blockIdx.x == 0) ? (0x80000000u - (nblocks - 1)) : 1u;
-    __threadfence();
-    unsigned old = atomicAdd(bar, inc);
-    unsigned long long polls = 0;
-    while (((old ^ ldAcquire(bar)) & 0x80000000u) == 0) {
-        if (++polls > spinLimit || ldVolatile(err) != 0) {
-            atomicOr(err, 1u);
-            return false;
+    const unsigned inc = (blockIdx.x == 0) ? (0x80000000u - (nblocks - 1)) : 1u;
+    __threadfence();  // release: this block's writes before its arrival
+    const unsigned old = atomicAdd(bar, inc);
+    // The block whose arrival flips the top bit is the last one and need not
+    // poll.  The others poll the barrier word alone (one round trip per poll)
+    // and look at the error word every 32 polls.
+    if ((((old + inc) ^ old) & 0x80000000u) == 0) {
+        unsigned long long polls = 0;
+        while (((old ^ ldVolatile(bar)) & 0x80000000u) == 0) {
+            ++polls;
+            if (polls > spinLimit || ((polls & 31u) == 0 && ldVolatile(err) != 0)) {
+                atomicOr(err, 1u);
+                return false;
+            }
+            if (polls > 64) __nanosleep(64);
         }
-        if (polls > 64) __nanosleep(64);
     }
-    __threadfence();
+    __threadfence();  // acquire: the other blocks' writes before their arrivals
     return ldVolatile(err) == 0;
 }
 
