@@ -164,6 +164,7 @@ def lib():
             "gb_selector_param_count": (C.c_size_t, []),
             "gb_bfs_set_selector": (C.c_int, [vp, C.c_int, vp, C.c_size_t]),
             "gb_bfs_hub_first": (C.c_int, [vp]),
+            "gb_bfs_graph": (C.c_int, [vp, P]),
             "gb_bfs_profile_levels": (C.c_int, [vp, C.c_uint32, C.POINTER(BfsOptions), C.c_int, _f32p, _f32p,
                                                 C.c_size_t, C.POINTER(C.c_size_t)]),
             "gb_bfs_profile_batch_levels": (C.c_int, [vp, _u32p, C.c_int, C.POINTER(BfsOptions), C.c_int, _f32p,
@@ -505,6 +506,10 @@ class GpuBfs:
 
     def lastLevels(self) -> int:
         return lib().gb_bfs_last_levels(self._h)
+
+    def graph(self) -> Graph:
+        """GpuBfs::graph(): the traversed graph, copied back from the device."""
+        return _make(lib().gb_bfs_graph, self._h)
 
     def hub_first(self):
         """Hub-first adjacency order on the device: same depths, bottom-up

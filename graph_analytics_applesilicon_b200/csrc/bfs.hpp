@@ -41,6 +41,7 @@ struct gb_bfs {
     std::vector<uint32_t> hostRowPtr;  // degrees of sources on the host
     gb::DevBuf<uint32_t> rowPtr, colIdx, dist;
     bool hubFirst = false;  // adjacency lists re-sorted hub-first (gb_bfs_hub_first)
+    uint32_t flags = 0;     // the graph's GGPUCSR1 flags when known (file handles)
     gb::Stream stream;
     gb::EventPair ev;
     gb::ScanScratch scan;

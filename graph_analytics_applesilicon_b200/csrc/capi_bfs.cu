@@ -1,6 +1,7 @@
 // capi_bfs.cu -- extern "C" entry points for graphs, BFS, primitives and the
 // selector (declared in include/graph_b200.h).  Every entry point catches the
 // library's exceptions and returns a gb_status; gb_last_error() holds the text.
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -227,6 +228,31 @@ int gb_bfs_create(const uint32_t* row_ptr, const uint32_t* col_idx, uint64_t n, 
         h->hstage.ensure(16);
         GB_CUDA(cudaStreamSynchronize(h->stream.s));
         *out = h.release();
+    });
+}
+
+int gb_bfs_graph(const gb_bfs* h, gb_csr* out) {
+    return guard([&] {
+        GB_REQUIRE(h && out, "null argument");
+        uint32_t* rp = static_cast<uint32_t*>(std::malloc((h->n + 1) * 4));
+        uint32_t* ci = static_cast<uint32_t*>(std::malloc(std::max<uint64_t>(h->m, 1) * 4));
+        if (!rp || !ci) {
+            std::free(rp);
+            std::free(ci);
+            throw Error(GB_ERR_OOM, "host allocation failed");
+        }
+        GB_CUDA(cudaStreamSynchronize(h->stream.s));
+        std::memcpy(rp, h->hostRowPtr.data(), (h->n + 1) * 4);
+        if (h->m && cudaMemcpy(ci, h->colIdx.get(), h->m * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            std::free(rp);
+            std::free(ci);
+            throw Error(GB_ERR_CUDA, "gb_bfs_graph: device-to-host copy failed");
+        }
+        out->n = h->n;
+        out->m = h->m;
+        out->flags = h->hubFirst ? (h->flags & ~GB_FLAG_SORTED) : h->flags;
+        out->row_ptr = rp;
+        out->col_idx = ci;
     });
 }
 

@@ -183,6 +183,7 @@ int gb_bfs_create_from_file(const char* path, gb_bfs** out, uint64_t* n_out, uin
         auto h = std::make_unique<gb_bfs>();
         h->n = b.n;
         h->m = b.m;
+        h->flags = b.flags;
         h->hostRowPtr.resize(b.n + 1);
         readParallel(b, h->hostRowPtr.data(), (b.n + 1) * 4, 32);
         GB_REQUIRE(h->hostRowPtr[0] == 0 && h->hostRowPtr[b.n] == b.m, "row_ptr must start at 0 and end at m");

@@ -251,6 +251,13 @@ uint32_t gb_bfs_last_levels(const gb_bfs* h);
 const uint32_t* gb_bfs_device_dist(const gb_bfs* h);
 /* The CUDA stream the handle launches on (cudaStream_t as void*). */
 void* gb_bfs_stream(const gb_bfs* h);
+/* GpuBfs::graph() (src/metal/bfs_gpu.hpp:39): the graph the handle traverses,
+ * as a host CSR (the reference returns a view of its unified-memory buffers;
+ * a discrete GPU copies the device arrays back).  Adjacency in the handle's
+ * order (hub-first after gb_bfs_hub_first, which drops GB_FLAG_SORTED); flags
+ * are the file's for gb_bfs_create_from_file handles, else 0.  Release with
+ * gb_csr_free. */
+int gb_bfs_graph(const gb_bfs* h, gb_csr* out);
 /* Hub-first adjacency (the reference's proposed "hub-first neighbor order
  * inside adjacency lists", docs/REPORT.md:386-398 and 743-744): re-sorts the
  * handle's device copy of every adjacency list by descending neighbour degree,

@@ -36,7 +36,16 @@ public:
     }
     // From a symmetric .bin file, streamed straight into GPU memory.
     explicit GpuBfs(const char* path) : n_(0) { check(gb_bfs_create_from_file(path, &h_, &n_, nullptr)); }
-    ~GpuBfs() { gb_bfs_destroy(h_); }
+    ~GpuBfs() {
+        gb_csr_free(&g_);
+        gb_bfs_destroy(h_);
+    }
+    // GpuBfs::graph(): the traversed graph as a host CSR, copied back once on
+    // first use (the reference's view of shared buffers; see gb_bfs_graph).
+    const gb_csr& graph() const {
+        if (!g_.row_ptr) check(gb_bfs_graph(h_, &g_));
+        return g_;
+    }
     GpuBfs(const GpuBfs&) = delete;
     GpuBfs& operator=(const GpuBfs&) = delete;
 
@@ -92,6 +101,7 @@ private:
     }
     gb_bfs* h_ = nullptr;
     uint64_t n_;
+    mutable gb_csr g_{};
 };
 
 // PrVariant / parsePrVariant (src/metal/pagerank_gpu.hpp:25, pagerank_gpu.mm:21-28).

@@ -68,3 +68,23 @@ def test_bfs_from_file_rejects(gb, tmp_path):
     rp[5], rp[6] = rp[6], rp[5]  # decreasing row_ptr
     with pytest.raises(gb.GraphError):
         gb.GpuBfs(gb.Graph(g.n, g.m, g.flags, rp, g.col_idx))
+
+
+def test_bfs_graph_view(gb, tmp_path):
+    """GpuBfs::graph() (src/metal/bfs_gpu.hpp:39; the reference's test checks
+    graph::equal(bfs.graph(), g), tests/test_main.cpp:510): the handle's graph
+    comes back equal to the one it was built from, in hub-first order after
+    hub_first(), and with the file's flags for a file handle."""
+    g = gb.gen.rmat(14, 16, False, 6)
+    b = gb.GpuBfs(g)
+    v = b.graph()
+    assert (v.n, v.m) == (g.n, g.m)
+    assert np.array_equal(v.row_ptr, g.row_ptr) and np.array_equal(v.col_idx, g.col_idx)
+    b.hub_first()
+    h = gb.hub_first_gpu(g)
+    w = b.graph()
+    assert np.array_equal(w.col_idx, h.col_idx) and not (w.flags & 2)
+    path = str(tmp_path / "g.bin")
+    gb.save(g, path)
+    f = gb.GpuBfs.from_file(path).graph()
+    assert f.equal(g)
