@@ -209,13 +209,16 @@ __device__ void pushTile(const BArgs& a, BSmem<NT>& sm, uint32_t item, uint32_t 
                 fu[k] = sm.f[o];
             }
         }
+        // the EPT pushes issued stage by stage (seen masks, then the ORs), so
+        // their round trips overlap
+        unsigned long long bits[EPT], old[EPT];
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) bits[k] = fu[k] ? (fu[k] & ~a.seen[u[k]]) : 0ull;
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) old[k] = bits[k] ? atomicOr(&a.nx[u[k]], bits[k]) : 1ull;
 #pragma unroll
         for (int k = 0; k < EPT; ++k) {
-            bool cand = false;
-            if (fu[k]) {
-                const unsigned long long bits = fu[k] & ~a.seen[u[k]];
-                if (bits) cand = atomicOr(&a.nx[u[k]], bits) == 0ull;
-            }
+            const bool cand = old[k] == 0ull;
             if (__any_sync(kFull, cand)) {
                 const uint32_t pos = warpAppend(cand, &cur->ccnt);
                 if (cand) a.cq[pos] = u[k];
@@ -231,19 +234,18 @@ __device__ void pushWarpItem(const BArgs& a, uint32_t item, uint32_t S, uint32_t
     if (idx >= S) return;  // warp-uniform
     const uint32_t st = a.qs[qc][idx], d = a.qd[qc][idx];
     const unsigned long long f = a.fr[qc][a.qv[qc][idx]];
-    for (uint32_t base = 0; base < d; base += 32) {
-        const uint32_t e = base + laneId();
-        bool cand = false;
-        if (e < d) {
-            const uint32_t u = a.col_idx[st + e];
-            const unsigned long long bits = f & ~a.seen[u];
-            if (bits && atomicOr(&a.nx[u], bits) == 0ull) {
-                cand = true;
-                const uint32_t pos = atomicAdd(&cur->ccnt, 1u);
-                a.cq[pos] = u;
-            }
+    for (uint32_t base = 0; base < d; base += 64) {  // two rounds per step: their pushes overlap
+        const uint32_t e0 = base + laneId(), e1 = e0 + 32;
+        const uint32_t u0 = e0 < d ? a.col_idx[st + e0] : 0u, u1 = e1 < d ? a.col_idx[st + e1] : 0u;
+        const unsigned long long b0 = e0 < d ? f & ~a.seen[u0] : 0ull, b1 = e1 < d ? f & ~a.seen[u1] : 0ull;
+        const unsigned long long o0 = b0 ? atomicOr(&a.nx[u0], b0) : 1ull, o1 = b1 ? atomicOr(&a.nx[u1], b1) : 1ull;
+        const bool c0 = o0 == 0ull, c1 = o1 == 0ull;
+        if (__any_sync(kFull, c0 || c1)) {
+            const uint32_t p0 = warpAppend(c0, &cur->ccnt);
+            if (c0) a.cq[p0] = u0;
+            const uint32_t p1 = warpAppend(c1, &cur->ccnt);
+            if (c1) a.cq[p1] = u1;
         }
-        (void)cand;
     }
 }
 
