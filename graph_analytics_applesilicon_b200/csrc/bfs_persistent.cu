@@ -416,26 +416,27 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
     uint64_t scout, toCheck, unexplored, reached;
     int lastStrat;
     if (a.startLevel == 0) {
+        // One pass writes the initial state with the source already placed
+        // (depth 0, visited, frontier bit), so a single grid barrier ends the
+        // prologue.  bm[2] needs no clearing: level 0 clears it.
+        const uint32_t src = a.source;
+        const uint32_t st = a.row_ptr[src], d = a.row_ptr[src + 1] - st;
         uint4* d4 = reinterpret_cast<uint4*>(a.dist);
-        for (uint64_t i = gtid; i < a.n / 4; i += gthreads) d4[i] = make_uint4(kInf, kInf, kInf, kInf);
-        for (uint64_t i = a.n / 4 * 4 + gtid; i < a.n; i += gthreads) a.dist[i] = kInf;
+        for (uint64_t i = gtid; i < a.n / 4; i += gthreads) {
+            const uint32_t z = i == src / 4 ? (src & 3) : 4u;  // lane of the source, if in this vector
+            d4[i] = make_uint4(z == 0 ? 0u : kInf, z == 1 ? 0u : kInf, z == 2 ? 0u : kInf, z == 3 ? 0u : kInf);
+        }
+        for (uint64_t i = a.n / 4 * 4 + gtid; i < a.n; i += gthreads) a.dist[i] = i == src ? 0u : kInf;
         for (uint64_t w = gtid; w < a.words; w += gthreads) {
             uint32_t pad = 0;
             if (w == a.words - 1 && (a.n & 31)) pad = ~((1u << (a.n & 31)) - 1u);  // bits past n read as visited
-            a.visited[w] = pad;
-            a.bm[0][w] = 0;
+            const uint32_t srcBit = w == (src >> 5) ? 1u << (src & 31) : 0u;
+            a.visited[w] = pad | srcBit;
+            a.bm[0][w] = srcBit;
             a.bm[1][w] = 0;
-            a.bm[2][w] = 0;
         }
-        if (gtid == 0)
-            for (int s = 0; s < 3; ++s) a.ctr[s] = GbPCounters{};
-        if (!gridBarrier(bar, err, a.spinLimit)) return;
-        const uint32_t src = a.source;
-        const uint32_t st = a.row_ptr[src], d = a.row_ptr[src + 1] - st;
         if (gtid == 0) {
-            a.dist[src] = 0;
-            a.visited[src >> 5] |= 1u << (src & 31);
-            a.bm[0][src >> 5] |= 1u << (src & 31);
+            for (int s = 0; s < 3; ++s) a.ctr[s] = GbPCounters{};
             GbPCounters& c = a.ctr[2];
             c.found = 1;
             c.nextEdges = d;
