@@ -418,15 +418,12 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
     if (a.startLevel == 0) {
         // One pass writes the initial state with the source already placed
         // (depth 0, visited, frontier bit), so a single grid barrier ends the
-        // prologue.  bm[2] needs no clearing: level 0 clears it.
+        // prologue.  bm[2] needs no clearing: level 0 clears it.  The depth
+        // array was set to infinity by a memset before the launch (the copy
+        // engine's fill is faster than the kernel's stores).
         const uint32_t src = a.source;
         const uint32_t st = a.row_ptr[src], d = a.row_ptr[src + 1] - st;
-        uint4* d4 = reinterpret_cast<uint4*>(a.dist);
-        for (uint64_t i = gtid; i < a.n / 4; i += gthreads) {
-            const uint32_t z = i == src / 4 ? (src & 3) : 4u;  // lane of the source, if in this vector
-            d4[i] = make_uint4(z == 0 ? 0u : kInf, z == 1 ? 0u : kInf, z == 2 ? 0u : kInf, z == 3 ? 0u : kInf);
-        }
-        for (uint64_t i = a.n / 4 * 4 + gtid; i < a.n; i += gthreads) a.dist[i] = i == src ? 0u : kInf;
+        if (gtid == 0) a.dist[src] = 0;  // the rest is already infinity (memset before the launch)
         for (uint64_t w = gtid; w < a.words; w += gthreads) {
             uint32_t pad = 0;
             if (w == a.words - 1 && (a.n & 31)) pad = ~((1u << (a.n & 31)) - 1u);  // bits past n read as visited
@@ -750,6 +747,7 @@ void gb_bfs::runPersistent(uint32_t src, const gb_bfs_options& o, std::vector<gb
         throw Error(GB_ERR_STATE, "learned selector requested but no parameters are loaded");
     GB_CUDA(cudaMemsetAsync(pctl.get(), 0, 4 * sizeof(unsigned), stream.s));
     GB_CUDA(cudaEventRecord(ev.a, stream.s));
+    GB_CUDA(cudaMemsetAsync(dist.get(), 0xFF, n * 4, stream.s));  // every depth infinity (0xFFFFFFFF)
     launchFor(*this, a);
     GB_CUDA(cudaEventRecord(ev.b, stream.s));
     unsigned ctl[4];
