@@ -505,7 +505,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
         // direction, reuses that decision (every block sees the same
         // counters, so all blocks reuse alike): long runs of similar levels
         // (a road graph's 1,800) then skip the evaluation.
-        bool useSel = a.force < 0 && learned;
+        // A frontier of at most 32 vertices runs the rule's top-down (its hubs
+        // are split by edges): every strategy costs about the same there, so
+        // the selector's evaluation would only add to the level.
+        bool useSel = a.force < 0 && learned && !(size <= 32 && !bottomUp);
         if (useSel) {
             const float lf = log2f(1.0f + (float)size), le = log2f(1.0f + (float)fedges);
             if (selLast >= 0 && bottomUp == selLastBU && fabsf(lf - selLastF) < 0.25f && fabsf(le - selLastE) < 0.25f) {
