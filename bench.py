@@ -16,7 +16,7 @@ source's component / time (src/bench/main.cpp:329-370).
               events on the library's stream around the 64 launches.
   e2e         the same call with a pinned host output buffer per source: the
               16.8 MB uint32 depth array comes back to the host inside the timed
-              region (over PCIe as 1 byte per depth, widened on the host).
+              region (over PCIe as 4 bits per depth, widened on the host).
   roofline    persistent kernel, HBM bound: graph-pass bytes 4(n+1)+4m+4n per
               traversal / mean launch time, against the measured copy peak.
   cpu_baseline the reference's own cpu_do (oracle/_ref, all host cores) on a
@@ -129,8 +129,10 @@ def build_graph(G, scale=SCALE, nsrc=NSRC, gpu_prep=True):
 
 
 def depth_wire_bytes(n, levels):
-    """Bytes per depth on the PCIe wire: the library packs depths to 1 or 2
-    bytes when the level count allows (arrays of 2^18 vertices or more)."""
+    """Bytes per depth on the PCIe wire: the library packs depths to 4 bits,
+    1 or 2 bytes when the level count allows (arrays of 2^18 vertices or more)."""
+    if n >= (1 << 18) and levels < 15:
+        return 0.5
     if n >= (1 << 18) and levels < 255:
         return 1
     if n >= (1 << 18) and levels < 65535:
@@ -353,7 +355,7 @@ def bfs_config_workload(args, world, rank, local):
                        "single_tuned": {"block": o1.block, "grid_blocks": o1.grid_blocks, "hub_min": o1.hub_min},
                        "parallelism": f"replicas{world}"},
             "e2e": {"value": world * e64 / (e2e * 1e-3) / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 256,
-                    "d2h_bytes_per_step": depth_wire_bytes(g.n, batch_levels) * 64 * g.n,
+                    "d2h_bytes_per_step": int(depth_wire_bytes(g.n, batch_levels) * 64 * g.n),
                     "result_bytes_per_step": 4 * 64 * g.n},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -765,7 +767,7 @@ def main():
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (CSR 293 MB)",
                    "edges_per_step": edges_per_step},
         "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),
-                "d2h_bytes_per_step": depth_wire_bytes(g.n, max_levels) * g.n * len(srcs),
+                "d2h_bytes_per_step": int(depth_wire_bytes(g.n, max_levels) * g.n * len(srcs)),
                 "result_bytes_per_step": 4 * g.n * len(srcs)},
         "gpu_launches": len(srcs) * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

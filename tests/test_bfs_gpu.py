@@ -163,13 +163,13 @@ def test_primitives_queue_bitmap_roundtrip(gb):
         assert np.array_equal(np.sort(q2), np.sort(q))
 
 
-@pytest.mark.parametrize("case", ["u8", "u16"])
+@pytest.mark.parametrize("case", ["u4", "u8", "u16"])
 def test_packed_depth_transfer(gb, oracle, case):
-    """Depths returned to host memory travel packed (1 or 2 bytes per vertex)
-    when the level count allows; arrays of at least 2^18 vertices with
+    """Depths returned to host memory travel packed (4 bits, 1 or 2 bytes per
+    vertex) when the level count allows; arrays of at least 2^18 vertices with
     unreached vertices, single and batched runs: every depth must equal the
     oracle's."""
-    if case == "u8":  # a power-law graph plus a separate path: low depths, unreached vertices
+    if case == "u4":  # a power-law graph plus a separate path: few levels, unreached vertices
         a = gb.gen.rmat(18, 8, False, 21)
         n = a.n + 20000
         rows = np.repeat(np.arange(a.n, dtype=np.uint32), np.diff(a.row_ptr.astype(np.int64)))
@@ -177,6 +177,8 @@ def test_packed_depth_transfer(gb, oracle, case):
         eu = np.concatenate([rows[keep], np.arange(a.n, n - 1, dtype=np.uint32)])
         ev = np.concatenate([a.col_idx[keep], np.arange(a.n + 1, n, dtype=np.uint32)])
         g = gb.from_edges(n, eu, ev, False)
+    elif case == "u8":  # a sparse random graph: 20-30 levels
+        g = gb.gen.chung_lu(300000, 2.8, 1.6, 24)
     else:  # a road grid: hundreds of levels
         g = gb.gen.road(560, 560, 0.04, 0.005, 22)
     og = oracle.HostGraph(g.n, g.m, g.flags, g.row_ptr, g.col_idx)
@@ -188,7 +190,8 @@ def test_packed_depth_transfer(gb, oracle, case):
         for variant in ("gpu_do_persistent", "gpu_do"):
             got = bfs.run(variant, int(s))
             assert np.array_equal(got, want), (case, variant, s)
-        assert (bfs.lastLevels() < 255) == (case == "u8")
+        L = bfs.lastLevels()
+        assert {"u4": L < 15, "u8": 15 <= L < 255, "u16": L >= 255}[case], (case, L)
     batch = bfs.run_batch(srcs)
     for i, s in enumerate(srcs):
         assert np.array_equal(batch[i], oracle.bfs_serial(og, int(s)))
