@@ -96,13 +96,6 @@ void gb_csr_free(gb_csr* g) {
     g->n = g->m = 0;
 }
 
-int gb_csr_save(const gb_csr* g, const char* path) {
-    return guard([&] {
-        GB_REQUIRE(path, "null path");
-        csrSave(fromC(g), path);
-    });
-}
-
 int gb_csr_validate(const gb_csr* g, char* msg, size_t cap) {
     return guard([&] {
         std::string e = csrValidate(fromC(g));

@@ -3,7 +3,8 @@
 // read it in place through unified memory).  A discrete GPU cannot do that,
 // so the ways in here keep the path from disk to HBM short:
 //   gb_csr_load          read by several threads (pread of disjoint slices)
-//                        straight into the returned arrays;
+//                        straight into the returned arrays (gb_csr_save
+//                        writes the same way);
 //   gb_csr_load_pinned   the arrays land in page-locked host memory, read by
 //                        several threads at once (pread of disjoint slices);
 //                        every later upload of them runs at full PCIe speed.
@@ -95,6 +96,28 @@ void readParallel(const BinFile& b, void* dst, uint64_t bytes, uint64_t off) {
     if (failed) throw Error(GB_ERR_IO, b.path + ": short read");
 }
 
+// Writes bytes from src at file offset off with up to 8 threads (pwrite of
+// kSlice slices).
+bool writeParallel(int fd, const void* src, uint64_t bytes, uint64_t off) {
+    const int64_t slices = (int64_t)((bytes + kSlice - 1) / kSlice);
+    const int threads = (int)std::max<int64_t>(1, std::min<int64_t>({8, slices, omp_get_max_threads()}));
+    bool failed = false;
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 1) reduction(|| : failed)
+    for (int64_t s = 0; s < slices; ++s) {
+        const uint64_t lo = (uint64_t)s * kSlice, len = std::min(kSlice, bytes - lo);
+        uint64_t put = 0;
+        while (put < len) {
+            const ssize_t r = pwrite(fd, static_cast<const char*>(src) + lo + put, len - put, (off_t)(off + lo + put));
+            if (r <= 0) {
+                failed = true;
+                break;
+            }
+            put += (uint64_t)r;
+        }
+    }
+    return !failed;
+}
+
 }  // namespace
 
 bool freePinnedArray(void* p) {
@@ -134,6 +157,29 @@ int gb_csr_load(const char* path, gb_csr* out) {
         out->flags = b.flags;
         out->row_ptr = rp;
         out->col_idx = ci;
+    });
+}
+
+// graph::save (src/graph/csr.cpp:30-44): header then row_ptr then col_idx,
+// written straight from the caller's arrays by several threads.
+int gb_csr_save(const gb_csr* g, const char* path) {
+    return guard([&] {
+        GB_REQUIRE(path, "null path");
+        GB_REQUIRE(g && g->row_ptr && (g->m == 0 || g->col_idx), "null graph");
+        const std::string p = path;
+        const int fd = open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+        if (fd < 0) throw Error(GB_ERR_IO, "cannot write " + p);
+        unsigned char hdr[32] = {};
+        std::memcpy(hdr, kBinMagic, 8);
+        const uint32_t version = 1;
+        std::memcpy(hdr + 8, &version, 4);
+        std::memcpy(hdr + 12, &g->flags, 4);
+        std::memcpy(hdr + 16, &g->n, 8);
+        std::memcpy(hdr + 24, &g->m, 8);
+        bool ok = writeParallel(fd, hdr, sizeof hdr, 0) && writeParallel(fd, g->row_ptr, (g->n + 1) * 4, 32) &&
+                  (g->m == 0 || writeParallel(fd, g->col_idx, g->m * 4, 32 + (g->n + 1) * 4));
+        ok = (close(fd) == 0) && ok;
+        if (!ok) throw Error(GB_ERR_IO, "short write to " + p);
     });
 }
 
