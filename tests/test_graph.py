@@ -90,6 +90,23 @@ def test_bin_roundtrip_and_rejects(gb):
             gb.load(bad)
         with pytest.raises(gb.GraphError):
             gb.load(os.path.join(d, "missing.bin"))
+        # a file whose size disagrees with its header, and a path that cannot be written
+        g = gb.gen.grid2d(10, 10)
+        p = os.path.join(d, "short.bin")
+        gb.save(g, p)
+        with open(p, "r+b") as f:
+            f.truncate(os.path.getsize(p) - 4)
+        with pytest.raises(gb.GraphError) as e:
+            gb.load(p)
+        assert e.value.status == 6 and "size does not match header" in str(e.value)
+        with pytest.raises(gb.GraphError) as e:
+            gb.save(g, os.path.join(d, "no_such_dir", "x.bin"))
+        assert e.value.status == 6
+        # a multi-slice graph (arrays larger than one 8 MiB read/write slice)
+        big = gb.gen.rmat(18, 16, False, 4)
+        p = os.path.join(d, "big.bin")
+        gb.save(big, p)
+        assert gb.load(p).equal(big)
 
 
 def test_benchmark_generators_shapes(gb):
