@@ -29,6 +29,7 @@ namespace {
 constexpr unsigned long long kHubShift = 40;
 constexpr unsigned long long kHubMask = (1ull << kHubShift) - 1;
 constexpr uint32_t kTraceCap = 1u << 16;
+constexpr uint64_t kEnqueueEdges = 1ull << 20;  // top-down levels with this many edges build no queue
 
 enum { S_LEVEL, S_BOTTOMUP, S_SCOUT, S_TOCHECK, S_UNEXPLORED, S_REACHED, S_QVALID, S_LAST, S_COUNT };
 
@@ -69,10 +70,13 @@ struct Acc {
 };
 
 // Append a claimed u (all 32 lanes call together) to the next frontier:
-// depth, bitmap bit, queue entry (degree < hub_min) or hub entry.
+// depth, bitmap bit and, when enq, a queue entry (degree < hub_min) or hub
+// entry.  Without enq the next level, if top-down, rebuilds its queue from
+// the bitmap (one block-aggregated append per block and round instead of one
+// atomic per warp here).
 __device__ __forceinline__ void appendClaimed(const PArgs& a, bool claimed, uint32_t u, uint32_t st, uint32_t en,
                                               uint32_t level, GbPCounters* cur, uint32_t* bmNext, uint32_t nq,
-                                              Acc& acc) {
+                                              Acc& acc, bool enq) {
     const uint32_t w = u >> 5, bit = 1u << (u & 31);
     if (!__any_sync(kFull, claimed)) return;
     const uint32_t d = claimed ? en - st : 0u;
@@ -82,6 +86,7 @@ __device__ __forceinline__ void appendClaimed(const PArgs& a, bool claimed, uint
         acc.found++;
         acc.deg += d;
     }
+    if (!enq) return;
     const bool hub = claimed && d >= a.hubMin;
     const bool q = claimed && !hub;
     if (__any_sync(kFull, q)) {
@@ -108,7 +113,8 @@ __device__ __forceinline__ void appendClaimed(const PArgs& a, bool claimed, uint
 // rather than run one claim after another.
 template <int K>
 __device__ __forceinline__ void discoverN(const PArgs& a, const bool* has, const uint32_t* u, uint32_t level,
-                                          GbPCounters* cur, uint32_t* bmNext, uint32_t nq, Acc& acc, bool precheck) {
+                                          GbPCounters* cur, uint32_t* bmNext, uint32_t nq, Acc& acc, bool precheck,
+                                          bool enq) {
     bool cand[K];
     uint32_t st[K], en[K], old[K];
 #pragma unroll
@@ -128,7 +134,7 @@ __device__ __forceinline__ void discoverN(const PArgs& a, const bool* has, const
     }
 #pragma unroll
     for (int k = 0; k < K; ++k)
-        appendClaimed(a, !(old[k] & (1u << (u[k] & 31))), u[k], st[k], en[k], level, cur, bmNext, nq, acc);
+        appendClaimed(a, !(old[k] & (1u << (u[k] & 31))), u[k], st[k], en[k], level, cur, bmNext, nq, acc, enq);
 }
 
 template <int NT>
@@ -172,7 +178,7 @@ __device__ __forceinline__ bool barrierWithCounters(const PArgs& a, Smem<NT>& sm
 // binary search over the staged offsets.
 template <int NT, int EPT>
 __device__ void tdTile(const PArgs& a, Smem<NT>& sm, uint32_t item, uint32_t S, uint32_t qc, uint32_t level,
-                       GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre) {
+                       GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre, bool enq) {
     const uint32_t idx = item * NT + threadIdx.x;
     uint32_t st = 0, d = 0;
     if (idx < S) {
@@ -199,7 +205,7 @@ __device__ void tdTile(const PArgs& a, Smem<NT>& sm, uint32_t item, uint32_t S, 
             }
         }
 #pragma unroll
-        discoverN<EPT>(a, has, u, level, cur, bmNext, qc ^ 1u, acc, pre);
+        discoverN<EPT>(a, has, u, level, cur, bmNext, qc ^ 1u, acc, pre, enq);
     }
     __syncthreads();
 }
@@ -211,7 +217,7 @@ __device__ void tdTile(const PArgs& a, Smem<NT>& sm, uint32_t item, uint32_t S, 
 // graphs, degree ~4, G = 8) thus use a quarter of the warps, so a quarter of
 // the queue appends, and most vertices still finish in one round.
 __device__ __forceinline__ void tdGroups(const PArgs& a, uint32_t S, unsigned G, uint32_t qc, uint32_t level,
-                                         GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre) {
+                                         GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre, bool enq) {
     const unsigned lane = laneId(), per = 32u / G;
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -224,7 +230,7 @@ __device__ __forceinline__ void tdGroups(const PArgs& a, uint32_t S, unsigned G,
             const uint32_t e = e0 + (lane & (G - 1));
             const bool he[2] = {e < d, e + G < d};
             const uint32_t u[2] = {he[0] ? a.col_idx[st + e] : 0u, he[1] ? a.col_idx[st + e + G] : 0u};
-            discoverN<2>(a, he, u, level, cur, bmNext, qc ^ 1u, acc, pre);
+            discoverN<2>(a, he, u, level, cur, bmNext, qc ^ 1u, acc, pre, enq);
         }
     }
 }
@@ -233,7 +239,7 @@ __device__ __forceinline__ void tdGroups(const PArgs& a, uint32_t S, unsigned G,
 // edges per thread per round so their loads overlap.
 template <int NT>
 __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e1, uint32_t H, uint32_t qc,
-                           uint32_t level, GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre) {
+                           uint32_t level, GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre, bool enq) {
     const unsigned long long* ho = a.ho[qc];
     if (threadIdx.x == 0) {
         uint32_t lo = ownerOf(ho, 0u, H - 1, (unsigned long long)e0);
@@ -256,7 +262,7 @@ __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e
             }
         }
 #pragma unroll
-        discoverN<2>(a, has, u, level, cur, bmNext, qc ^ 1u, acc, pre);
+        discoverN<2>(a, has, u, level, cur, bmNext, qc ^ 1u, acc, pre, enq);
     }
     __syncthreads();
 }
@@ -573,6 +579,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
             const uint32_t qc = level & 1u;
             const uint32_t H = (uint32_t)(hp >> kHubShift);
             const uint64_t HE = hp & kHubMask;
+            // a level with many edges to expand skips the queue appends: its
+            // successor is most often bottom-up (no queue), and a top-down one
+            // rebuilds the queue from the bitmap
+            const bool enq = fedges < kEnqueueEdges;
             // warp per vertex: a static warp-strided loop over the queue (no
             // tickets, no block barriers); edge-balanced tiles: block tickets
             const bool warpMode = strat == GB_STRAT_TD_WARP;
@@ -581,7 +591,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
                 // group of at least twice the mean degree: most vertices take one round
                 const uint64_t want = S ? 2 * ((qEdges + S - 1) / S) : 1;
                 const unsigned G = want <= 4 ? 4u : want <= 8 ? 8u : want <= 16 ? 16u : 32u;
-                tdGroups(a, S, G, qc, level, cur, a.bm[(level + 1) % 3], acc, fedges >= 65536);
+                tdGroups(a, S, G, qc, level, cur, a.bm[(level + 1) % 3], acc, fedges >= 65536, enq);
             }
             const uint32_t nt = warpMode ? 0u : (S + NT - 1) / NT;
             const uint64_t HC = (uint64_t)NT * 2;
@@ -597,13 +607,13 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
                 if (item >= nt + nh) break;
                 if (item < nt) {
                     switch (strat) {
-                        case GB_STRAT_TD_EPT1: tdTile<NT, 1>(a, sm, item, S, qc, level, cur, bmNext, acc, pre); break;
-                        case GB_STRAT_TD_EPT4: tdTile<NT, 4>(a, sm, item, S, qc, level, cur, bmNext, acc, pre); break;
-                        default: tdTile<NT, 2>(a, sm, item, S, qc, level, cur, bmNext, acc, pre); break;
+                        case GB_STRAT_TD_EPT1: tdTile<NT, 1>(a, sm, item, S, qc, level, cur, bmNext, acc, pre, enq); break;
+                        case GB_STRAT_TD_EPT4: tdTile<NT, 4>(a, sm, item, S, qc, level, cur, bmNext, acc, pre, enq); break;
+                        default: tdTile<NT, 2>(a, sm, item, S, qc, level, cur, bmNext, acc, pre, enq); break;
                     }
                 } else {
                     const uint64_t e0 = (uint64_t)(item - nt) * HC;
-                    tdHubChunk<NT>(a, sm, e0, min(e0 + HC, HE), H, qc, level, cur, bmNext, acc, pre);
+                    tdHubChunk<NT>(a, sm, e0, min(e0 + HC, HE), H, qc, level, cur, bmNext, acc, pre, enq);
                 }
             }
         }
@@ -641,7 +651,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
         } else {
             scout = nextE;
         }
-        qValid = strat != GB_STRAT_BU;
+        qValid = strat != GB_STRAT_BU && fedges < kEnqueueEdges;
         lastStrat = strat;
         ++level;
     }
