@@ -29,7 +29,7 @@ namespace {
 constexpr unsigned long long kHubShift = 40;
 constexpr unsigned long long kHubMask = (1ull << kHubShift) - 1;
 constexpr uint32_t kTraceCap = 1u << 16;
-constexpr uint64_t kEnqueueEdges = 1ull << 20;  // top-down levels with this many edges build no queue
+constexpr uint64_t kEnqueueEdges = 1ull << 18;  // top-down levels with this many edges build no queue
 
 enum { S_LEVEL, S_BOTTOMUP, S_SCOUT, S_TOCHECK, S_UNEXPLORED, S_REACHED, S_QVALID, S_LAST, S_COUNT };
 
