@@ -156,6 +156,8 @@ def lib():
                                      C.POINTER(C.c_size_t)]),
             "gb_bfs_run_batch": (C.c_int, [vp, _u32p, C.c_int, vp, C.POINTER(BfsOptions), vp, C.c_size_t,
                                            C.POINTER(C.c_size_t)]),
+            "gb_bfs_run_many": (C.c_int, [vp, C.c_int, _u32p, C.c_uint32, vp, C.c_uint64, C.POINTER(BfsOptions),
+                                          vp, vp]),
             "gb_bfs_last_gpu_ms": (C.c_double, [vp]),
             "gb_bfs_last_levels": (C.c_uint32, [vp]),
             "gb_bfs_device_dist": (vp, [vp]),
@@ -500,6 +502,31 @@ class GpuBfs:
         check(lib().gb_bfs_run_batch(self._h, src, src.size, out.ctypes.data, C.byref(o),
                                      C.cast(buf, C.c_void_p) if trace else None, cap, C.byref(nlev)))
         return (out, _levels(buf, nlev.value)) if trace else out
+
+    def run_many(self, variant, sources, out=None, stride=None, opts: BfsOptions | None = None, device=False):
+        """One traversal per source in one call (gb_bfs_run_many); returns
+        (depths, gpu_ms[k], levels[k]).  depths: uint32[k, n] (out, or a new
+        array), or out itself when stride is 0 (it ends with the last source's
+        depths); device=True keeps every result on the GPU (depths None)."""
+        v = BFS_VARIANTS[variant] if isinstance(variant, str) else int(variant)
+        src = np.ascontiguousarray(sources, np.uint32)
+        o = opts if opts is not None else BfsOptions()
+        ms = np.zeros(src.size, np.float32)
+        lv = np.zeros(src.size, np.uint32)
+        if device:
+            out, stride, ptr = None, 0, None
+        else:
+            if out is None:
+                out = np.empty((src.size, self.n), np.uint32)
+            if stride is None:
+                stride = self.n if out.size >= src.size * self.n else 0
+            need = (src.size - 1) * stride + self.n if src.size else 0
+            if out.dtype != np.uint32 or not out.flags.c_contiguous or out.size < need:
+                raise ValueError(f"out must be a contiguous uint32 array of at least {need} entries")
+            ptr = out.ctypes.data
+        check(lib().gb_bfs_run_many(self._h, v, src, src.size, ptr, stride, C.byref(o), ms.ctypes.data,
+                                    lv.ctypes.data))
+        return out, ms, lv
 
     def lastGpuMs(self) -> float:
         return lib().gb_bfs_last_gpu_ms(self._h)

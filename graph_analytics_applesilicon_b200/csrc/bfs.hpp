@@ -34,6 +34,15 @@ namespace gb {
 // Copies count depths from device d to host out (uint32, unreached ~0), packed
 // to 1 or 2 bytes per depth over PCIe when `levels` allows (depth_out.cu).
 void copyDepthsToHost(gb_bfs* h, const uint32_t* d, uint64_t count, uint32_t* out, uint32_t levels);
+// The same packing as stages of a pipeline: packFormat picks the width for a
+// traversal of `levels` levels (0: 4 bits, 1: 1 byte, 2: 2 bytes per depth;
+// -1: send uint32), enqueuePack packs on `st` (sets *overflow when a depth does
+// not fit), widenPacked turns the copied bytes back into uint32 on the host.
+int packFormat(uint64_t count, uint32_t levels);
+uint64_t packedBytes(int fmt, uint64_t count);
+void enqueuePack(int fmt, const uint32_t* d, uint64_t count, uint8_t* dev, unsigned* overflow, cudaStream_t st);
+void widenPacked(int fmt, const uint8_t* in, uint64_t count, uint32_t* out);
+constexpr int kManySlots = 3;  // depth buffers in flight in gb_bfs::runPersistentMany
 }  // namespace gb
 
 struct gb_bfs {
@@ -81,8 +90,20 @@ struct gb_bfs {
     gb::DevBuf<unsigned> packFlag;
     gb::HostPinned<unsigned> packFlagHost;
     std::vector<cudaEvent_t> packEv;
+
+    // several sources per call (runPersistentMany): depth buffers besides
+    // dist, per-slot packed copies, per-source control words and events
+    gb::DevBuf<uint32_t> mDist[gb::kManySlots - 1];
+    gb::DevBuf<uint8_t> mPackDev[gb::kManySlots];
+    gb::HostPinned<uint8_t> mPackHost[gb::kManySlots];
+    gb::DevBuf<unsigned> mCtl, mFlag;
+    gb::HostPinned<unsigned> mCtlHost, mFlagHost;
+    std::vector<cudaEvent_t> mEv, mSlotEv;
+    gb::Stream copyStream;
     ~gb_bfs() {
         for (cudaEvent_t e : packEv) cudaEventDestroy(e);
+        for (cudaEvent_t e : mEv) cudaEventDestroy(e);
+        for (cudaEvent_t e : mSlotEv) cudaEventDestroy(e);
     }
 
     double lastGpuMs = 0;
@@ -97,6 +118,8 @@ struct gb_bfs {
     void runDirOpt(uint32_t src, const gb_bfs_options& o, std::vector<gb_level>* tr);
     void runPersistent(uint32_t src, const gb_bfs_options& o, std::vector<gb_level>* tr);
     void runBatch(const uint32_t* src, int k, const gb_bfs_options& o, std::vector<gb_level>* tr);
+    void runPersistentMany(const uint32_t* src, uint32_t count, uint32_t* out, uint64_t stride,
+                           const gb_bfs_options& o, float* ms, uint32_t* levels);
     // Profiling (selector training data).
     size_t profileLevels(uint32_t src, const gb_bfs_options& o, int repeats, float* feats, float* times,
                          size_t cap);

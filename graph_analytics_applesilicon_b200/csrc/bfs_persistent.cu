@@ -778,6 +778,128 @@ void gb_bfs::runPersistent(uint32_t src, const gb_bfs_options& o, std::vector<gb
     }
 }
 
+// Several sources in one call.  Traversal i writes depth buffer i % kManySlots
+// (dist, then mDist[]) and its own four control words (all zeroed by one
+// memset), so the traversals follow one another on the stream with no host
+// round trip between them.  With a host output, traversal i's depths are
+// packed on the stream right behind it (the width predicted from the most
+// levels seen so far; a depth that does not fit raises the overflow flag),
+// copied to pinned memory on the copy stream, and widened by host threads
+// while the next traversals run.  The host finishes source i before it queues
+// traversal i + kManySlots, the next user of slot i % kManySlots, so an
+// overflowing source can still be copied whole from its depth buffer.
+void gb_bfs::runPersistentMany(const uint32_t* src, uint32_t count, uint32_t* out, uint64_t stride,
+                               const gb_bfs_options& o, float* msOut, uint32_t* levelsOut) {
+    validateOptions(o);
+    ensurePersistent(o);
+    if (o.selector == GB_SELECT_LEARNED && !selLoaded[0])
+        throw Error(GB_ERR_STATE, "learned selector requested but no parameters are loaded");
+    if (count == 0) return;
+    for (auto& d : mDist) d.ensure(n + 4);
+    for (int s = 0; s < kManySlots; ++s) {  // sized for the widest packed form up front
+        mPackDev[s].ensure(2 * n + 16);
+        mPackHost[s].ensure(2 * n + 16);
+    }
+    mCtl.ensure((size_t)count * 4);
+    mCtlHost.ensure((size_t)count * 4);
+    mFlag.ensure(kManySlots);
+    mFlagHost.ensure(count);
+    while (mEv.size() < 2 * (size_t)count) {
+        cudaEvent_t e;
+        GB_CUDA(cudaEventCreate(&e));
+        mEv.push_back(e);
+    }
+    while (mSlotEv.size() < 2 * (size_t)kManySlots) {
+        cudaEvent_t e;
+        GB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        mSlotEv.push_back(e);
+    }
+    uint32_t* bufs[kManySlots];
+    bufs[0] = dist.get();
+    for (int s = 1; s < kManySlots; ++s) bufs[s] = mDist[s - 1].get();
+    std::vector<int> fmt(count, -1);
+    // packed width: from the most levels among this call's finished sources,
+    // else the handle's last run, else one byte per depth
+    uint32_t maxSeen = 0;
+    bool anySeen = false;
+    const bool timed = msOut != nullptr;
+    cudaStream_t st = stream.s, cs = copyStream.s;
+
+    GB_CUDA(cudaMemsetAsync(mCtl.get(), 0, (size_t)count * 4 * sizeof(unsigned), st));
+    auto enqueue = [&](uint32_t i) {
+        const int s = (int)(i % kManySlots);
+        PArgs a = makeArgs(*this, o, src[i]);
+        a.dist = bufs[s];
+        a.ctl = mCtl.get() + 4 * (size_t)i;
+        if (timed || i + 1 == count) GB_CUDA(cudaEventRecord(mEv[2 * i], st));
+        GB_CUDA(cudaMemsetAsync(bufs[s], 0xFF, n * 4, st));  // every depth infinity
+        launchFor(*this, a);
+        if (timed || i + 1 == count) GB_CUDA(cudaEventRecord(mEv[2 * i + 1], st));
+        if (!out) return;
+        cudaEvent_t packed = mSlotEv[s], copied = mSlotEv[kManySlots + s];
+        fmt[i] = packFormat(n, anySeen ? maxSeen : lastLevels ? lastLevels : 254);
+        if (fmt[i] >= 0) {
+            // the slot's previous copy must have left mPackDev[s]
+            if (i >= (uint32_t)kManySlots) GB_CUDA(cudaStreamWaitEvent(st, copied, 0));
+            GB_CUDA(cudaMemsetAsync(mFlag.get() + s, 0, sizeof(unsigned), st));
+            enqueuePack(fmt[i], bufs[s], n, mPackDev[s].get(), mFlag.get() + s, st);
+        }
+        GB_CUDA(cudaEventRecord(packed, st));
+        GB_CUDA(cudaStreamWaitEvent(cs, packed, 0));
+        if (fmt[i] >= 0) {
+            GB_CUDA(cudaMemcpyAsync(mPackHost[s].p, mPackDev[s].get(), packedBytes(fmt[i], n),
+                                    cudaMemcpyDeviceToHost, cs));
+            GB_CUDA(cudaMemcpyAsync(mFlagHost.p + i, mFlag.get() + s, sizeof(unsigned), cudaMemcpyDeviceToHost, cs));
+        }
+        GB_CUDA(cudaMemcpyAsync(mCtlHost.p + 4 * (size_t)i, mCtl.get() + 4 * (size_t)i, 4 * sizeof(unsigned),
+                                cudaMemcpyDeviceToHost, cs));
+        GB_CUDA(cudaEventRecord(copied, cs));
+    };
+    auto timeout = [&]() {
+        cudaStreamSynchronize(st);
+        cudaStreamSynchronize(cs);
+        return Error(GB_ERR_TIMEOUT, "persistent BFS: grid barrier wait exceeded its spin limit");
+    };
+
+    uint32_t queued = 0;
+    if (!out) {
+        for (; queued < count; ++queued) enqueue(queued);
+        GB_CUDA(cudaMemcpyAsync(mCtlHost.p, mCtl.get(), (size_t)count * 4 * sizeof(unsigned),
+                                cudaMemcpyDeviceToHost, st));
+    } else {
+        for (uint32_t i = 0; i < count; ++i) {
+            for (; queued < count && queued < i + (uint32_t)kManySlots; ++queued) enqueue(queued);
+            const int s = (int)(i % kManySlots);
+            GB_CUDA(cudaEventSynchronize(mSlotEv[kManySlots + s]));
+            const unsigned* c = mCtlHost.p + 4 * (size_t)i;
+            if (c[1]) throw timeout();
+            maxSeen = std::max(maxSeen, c[2]);
+            anySeen = true;
+            uint32_t* dst = out + (uint64_t)i * stride;
+            if (fmt[i] >= 0 && mFlagHost.p[i] == 0) {
+                widenPacked(fmt[i], mPackHost[s].p, n, dst);
+            } else {  // too many levels for the predicted width: the buffer is still intact
+                GB_CUDA(cudaMemcpyAsync(dst, bufs[s], n * 4, cudaMemcpyDeviceToHost, st));
+                GB_CUDA(cudaStreamSynchronize(st));
+            }
+        }
+    }
+    GB_CUDA(cudaStreamSynchronize(st));
+    GB_CUDA(cudaStreamSynchronize(cs));
+    for (uint32_t i = 0; i < count; ++i)
+        if (mCtlHost.p[4 * (size_t)i + 1]) throw timeout();
+    for (uint32_t i = 0; i < count; ++i) {
+        if (levelsOut) levelsOut[i] = mCtlHost.p[4 * (size_t)i + 2];
+        if (timed) GB_CUDA(cudaEventElapsedTime(&msOut[i], mEv[2 * i], mEv[2 * i + 1]));
+    }
+    float last = 0;
+    GB_CUDA(cudaEventElapsedTime(&last, mEv[2 * (count - 1)], mEv[2 * (count - 1) + 1]));
+    lastGpuMs = last;
+    lastLevels = mCtlHost.p[4 * (size_t)(count - 1) + 2];
+    const int lastSlot = (int)((count - 1) % kManySlots);
+    if (lastSlot) dist.swap(mDist[lastSlot - 1]);  // dist holds the last source's depths
+}
+
 // Selector training data.  A level's vertex set does not depend on the
 // strategy that ran the earlier levels, so running the whole BFS once per
 // strategy (forced at every level, alpha/beta rule off) gives every level's

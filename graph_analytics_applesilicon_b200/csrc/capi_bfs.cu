@@ -295,6 +295,37 @@ int gb_bfs_run(gb_bfs* h, int variant, uint32_t source, uint32_t* out_host, cons
     });
 }
 
+int gb_bfs_run_many(gb_bfs* h, int variant, const uint32_t* sources, uint32_t count, uint32_t* out_host,
+                    uint64_t stride, const gb_bfs_options* opt, float* gpu_ms, uint32_t* levels) {
+    return guard([&] {
+        GB_REQUIRE(h, "null handle");
+        GB_REQUIRE(count == 0 || sources, "null sources");
+        GB_REQUIRE(stride == 0 || stride >= h->n, "stride must be 0 or at least n");
+        for (uint32_t i = 0; i < count; ++i) GB_REQUIRE(sources[i] < h->n, "source out of range");
+        gb_bfs_options o;
+        gb_bfs_default_options(&o);
+        if (opt) o = *opt;
+        validateOptions(o);
+        if (variant == GB_BFS_PERSISTENT) {
+            h->runPersistentMany(sources, count, out_host, stride, o, gpu_ms, levels);
+            return;
+        }
+        for (uint32_t i = 0; i < count; ++i) {
+            switch (variant) {
+                case GB_BFS_VERTEX: h->runVertex(sources[i], o, nullptr); break;
+                case GB_BFS_NAIVE: h->runNaive(sources[i], o, nullptr); break;
+                case GB_BFS_BINNED: h->runBinned(sources[i], o, nullptr); break;
+                case GB_BFS_EDGE: h->runEdge(sources[i], o, nullptr); break;
+                case GB_BFS_DO: h->runDirOpt(sources[i], o, nullptr); break;
+                default: throw Error(GB_ERR_ARG, "unknown BFS variant " + std::to_string(variant));
+            }
+            if (out_host) copyDepthsToHost(h, h->dist.get(), h->n, out_host + (uint64_t)i * stride, h->lastLevels);
+            if (gpu_ms) gpu_ms[i] = (float)h->lastGpuMs;
+            if (levels) levels[i] = h->lastLevels;
+        }
+    });
+}
+
 double gb_bfs_last_gpu_ms(const gb_bfs* h) { return h ? h->lastGpuMs : -1.0; }
 uint32_t gb_bfs_last_levels(const gb_bfs* h) { return h ? h->lastLevels : 0; }
 const uint32_t* gb_bfs_device_dist(const gb_bfs* h) { return h ? h->dist.get() : nullptr; }

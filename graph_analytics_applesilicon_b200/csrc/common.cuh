@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 #include "graph_b200.h"
 
@@ -58,6 +59,10 @@ struct DevBuf {
         n = bytes / sizeof(T);
     }
     T* get() const { return p; }
+    void swap(DevBuf& o) {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+    }
 };
 
 // Pinned host allocation.

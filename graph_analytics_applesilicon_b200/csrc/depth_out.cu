@@ -138,6 +138,32 @@ bool packedCopy4(gb_bfs* h, const uint32_t* d, uint64_t count, uint32_t* out) {
 
 }  // namespace
 
+int packFormat(uint64_t count, uint32_t levels) {
+    if (count < kPackMin) return -1;
+    if (levels < 15) return 0;
+    if (levels < 255) return 1;
+    if (levels < 65535) return 2;
+    return -1;
+}
+
+uint64_t packedBytes(int fmt, uint64_t count) {
+    return fmt == 0 ? (count + 1) / 2 : fmt == 1 ? count : 2 * count;
+}
+
+void enqueuePack(int fmt, const uint32_t* d, uint64_t count, uint8_t* dev, unsigned* overflow, cudaStream_t st) {
+    const int grid = deviceSmCount() * 8;
+    if (fmt == 0) packDepths4Kernel<<<grid, 256, 0, st>>>(d, count, dev, overflow);
+    else if (fmt == 1) packDepthsKernel<uint8_t><<<grid, 256, 0, st>>>(d, count, dev, overflow);
+    else packDepthsKernel<uint16_t><<<grid, 256, 0, st>>>(d, count, reinterpret_cast<uint16_t*>(dev), overflow);
+    GB_LAUNCH_CHECK();
+}
+
+void widenPacked(int fmt, const uint8_t* in, uint64_t count, uint32_t* out) {
+    if (fmt == 0) widen4(in, out, count);
+    else if (fmt == 1) widen(in, out, count);
+    else widen(reinterpret_cast<const uint16_t*>(in), out, count);
+}
+
 void copyDepthsToHost(gb_bfs* h, const uint32_t* d, uint64_t count, uint32_t* out, uint32_t levels) {
     bool done = false;
     if (count >= kPackMin) {

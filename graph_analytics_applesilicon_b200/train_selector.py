@@ -1,7 +1,7 @@
 """Trains the learned per-level BFS strategy selector on the GPU.
 
   python -m graph_analytics_applesilicon_b200.train_selector generate OUT.npz
-  python -m graph_analytics_applesilicon_b200.train_selector train DATA.npz [OUT.npy]
+  python -m graph_analytics_applesilicon_b200.train_selector train DATA.npz [OUT.npy] [--seed S]
   python -m graph_analytics_applesilicon_b200.train_selector evaluate [PARAMS.npy]
   python -m graph_analytics_applesilicon_b200.train_selector generate-batch OUT.npz
   python -m graph_analytics_applesilicon_b200.train_selector train-batch DATA.npz
@@ -17,6 +17,8 @@ times.
 train: the MLP (8 features -> 32 -> 32 -> 5 predicted log2 us) is fitted with
 the library's GPU training kernels (gb_mlp_train, Adam) and written to
 selector_single.npy beside this file, where GpuBfs users and bench.py find it.
+--seed picks the initial weights and the minibatch order (default 0); the
+shipped selector_single.npy was trained with --seed 1.
 evaluate: learned vs rule persistent BFS on held-out graphs (same depths).
 
 Every handle uses the hub-first adjacency layout (GpuBfs.hub_first), the one
@@ -202,15 +204,20 @@ def evaluate_batch(params_path=None, batches=2):
 
 if __name__ == "__main__":
     sys.argv = [a for a in sys.argv if a != "--natural"]
+    seed = 0
+    if "--seed" in sys.argv:
+        i = sys.argv.index("--seed")
+        seed = int(sys.argv[i + 1])
+        del sys.argv[i:i + 2]
     cmd = sys.argv[1] if len(sys.argv) > 1 else "evaluate"
     if cmd == "generate":
         generate(sys.argv[2])
     elif cmd == "train":
-        train(sys.argv[2], sys.argv[3] if len(sys.argv) > 3 else None)
+        train(sys.argv[2], sys.argv[3] if len(sys.argv) > 3 else None, seed=seed)
     elif cmd == "generate-batch":
         generate_batch(sys.argv[2])
     elif cmd == "train-batch":
-        train(sys.argv[2], sys.argv[3] if len(sys.argv) > 3 else os.path.join(PKG, "selector_batch.npy"))
+        train(sys.argv[2], sys.argv[3] if len(sys.argv) > 3 else os.path.join(PKG, "selector_batch.npy"), seed=seed)
     elif cmd == "evaluate-batch":
         evaluate_batch(sys.argv[2] if len(sys.argv) > 2 else None)
     else:

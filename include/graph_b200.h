@@ -237,6 +237,20 @@ int gb_bfs_create_from_file(const char* path, gb_bfs** out, uint64_t* n_out, uin
  * trace: optional per-level records (cap entries, *nlev = levels run). */
 int gb_bfs_run(gb_bfs* h, int variant, uint32_t source, uint32_t* out_host,
                const gb_bfs_options* opt, gb_level* trace, size_t cap, size_t* nlev);
+/* The per-source loop of gbench (src/bench/main.cpp:324-364: one run per
+ * source, each timed) as one call.  For GB_BFS_PERSISTENT the traversals
+ * follow one another on the handle's stream with no host round trip between
+ * them; with out_host, the depths of traversal i are packed on the device,
+ * copied to the host on a second stream and widened there while the next
+ * traversals run.  Other variants run the sources one by one as gb_bfs_run.
+ * out_host: source i writes n entries at out_host + i * stride (stride 0:
+ * every source writes the same n entries, which end with the last source's
+ * depths; else stride >= n), or NULL (the last source's depths stay on the
+ * device, gb_bfs_device_dist, whose pointer may change with this call).
+ * gpu_ms, levels (each may be NULL): count entries, device time and level
+ * count of each traversal.  Every source is checked before any runs. */
+int gb_bfs_run_many(gb_bfs* h, int variant, const uint32_t* sources, uint32_t count, uint32_t* out_host,
+                    uint64_t stride, const gb_bfs_options* opt, float* gpu_ms, uint32_t* levels);
 /* 64-source batched BFS in one persistent launch (replaces the per-source loop
  * of src/bench/main.cpp:324-364).  k <= 64 sources; out_host: k * n entries,
  * source-major (out_host[i * n + v] = depth of v from sources[i]), or NULL. */
@@ -247,7 +261,8 @@ int gb_bfs_run_batch(gb_bfs* h, const uint32_t* sources, int k, uint32_t* out_ho
 double gb_bfs_last_gpu_ms(const gb_bfs* h);
 uint32_t gb_bfs_last_levels(const gb_bfs* h);
 /* Device pointer of the last single-source result (n uint32), for callers that
- * keep results on the GPU (GpuBfs::dist(), src/metal/bfs_gpu.hpp:40). */
+ * keep results on the GPU (GpuBfs::dist(), src/metal/bfs_gpu.hpp:40); read it
+ * again after gb_bfs_run_many, which may move the result to another buffer. */
 const uint32_t* gb_bfs_device_dist(const gb_bfs* h);
 /* The CUDA stream the handle launches on (cudaStream_t as void*). */
 void* gb_bfs_stream(const gb_bfs* h);

@@ -81,6 +81,18 @@ public:
                                buf.size(), &nl));
         if (tr) tr->assign(buf.begin(), buf.begin() + (long)nl);
     }
+    // One traversal per source in one call (the persistent variant queues them
+    // back to back and overlaps each result's copy with the next traversal);
+    // out: sources.size() * stride depths (stride 0: one n-entry buffer that
+    // ends with the last source's), or null to keep the last result on the device.
+    void runMany(int variant, const std::vector<uint32_t>& sources, uint32_t* out, uint64_t stride,
+                 const GpuBfsOptions& o, std::vector<float>* gpuMs = nullptr,
+                 std::vector<uint32_t>* levels = nullptr) {
+        if (gpuMs) gpuMs->assign(sources.size(), 0.0f);
+        if (levels) levels->assign(sources.size(), 0);
+        check(gb_bfs_run_many(h_, variant, sources.data(), (uint32_t)sources.size(), out, stride, &o,
+                              gpuMs ? gpuMs->data() : nullptr, levels ? levels->data() : nullptr));
+    }
     void setSelector(int which, const std::vector<float>& params) {
         check(gb_bfs_set_selector(h_, which, params.data(), params.size()));
     }
