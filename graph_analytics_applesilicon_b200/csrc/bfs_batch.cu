@@ -253,10 +253,10 @@ template <int NT>
 __device__ void pushHubChunk(const BArgs& a, BSmem<NT>& sm, uint64_t e0, uint64_t e1, uint32_t H, uint32_t qc,
                              BCounters* cur) {
     const unsigned long long* ho = a.ho[qc];
-    if (threadIdx.x == 0) {
-        const uint32_t lo = ownerOf(ho, 0u, H - 1, (unsigned long long)e0);
-        sm.range[0] = lo;
-        sm.range[1] = ownerOf(ho, lo, H - 1, (unsigned long long)(e1 - 1));
+    if (threadIdx.x < 64) {  // the chunk's first and last owners: warp 0 and warp 1 side by side
+        const unsigned long long key = threadIdx.x < 32 ? e0 : e1 - 1;
+        const uint32_t o = warpOwnerOf(ho, 0u, H - 1, key);
+        if ((threadIdx.x & 31u) == 0) sm.range[threadIdx.x >> 5] = o;
     }
     __syncthreads();
     const uint32_t lo = sm.range[0], hi = sm.range[1];

@@ -175,10 +175,13 @@ __device__ __forceinline__ bool barrierWithCounters(const PArgs& a, Smem<NT>& sm
 // Edge-balanced expansion of one tile of NT queue entries: the entries'
 // degrees are scanned in shared memory and every thread takes EPT edges per
 // round (thread t: edges base + k*NT + t), owner found by a shared-memory
-// binary search over the staged offsets.
+// binary search over the staged offsets.  The block expands part `part` of
+// `parts` equal slices of the tile's edges (a tile of high-degree entries is
+// split over several blocks; each scans the tile's degrees itself).
 template <int NT, int EPT>
 __device__ void tdTile(const PArgs& a, Smem<NT>& sm, uint32_t item, uint32_t S, uint32_t qc, uint32_t level,
-                       GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre, bool enq) {
+                       GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre, bool enq, uint32_t part,
+                       uint32_t parts) {
     const uint32_t idx = item * NT + threadIdx.x;
     uint32_t st = 0, d = 0;
     if (idx < S) {
@@ -191,13 +194,14 @@ __device__ void tdTile(const PArgs& a, Smem<NT>& sm, uint32_t item, uint32_t S, 
     sm.st[threadIdx.x] = st;
     __syncthreads();
     const uint32_t cnt = min((uint32_t)NT, S - item * NT);
-    for (uint32_t base = 0; base < tot; base += NT * EPT) {
+    const uint32_t lo = (uint32_t)((uint64_t)tot * part / parts), hi = (uint32_t)((uint64_t)tot * (part + 1) / parts);
+    for (uint32_t base = lo; base < hi; base += NT * EPT) {
         uint32_t u[EPT];
         bool has[EPT];
 #pragma unroll
         for (int k = 0; k < EPT; ++k) {
             const uint32_t e = base + k * NT + threadIdx.x;
-            has[k] = e < tot;
+            has[k] = e < hi;
             u[k] = 0;
             if (has[k]) {
                 const uint32_t o = ownerOf(sm.off, 0u, cnt - 1, e);
@@ -241,10 +245,10 @@ template <int NT>
 __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e1, uint32_t H, uint32_t qc,
                            uint32_t level, GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre, bool enq) {
     const unsigned long long* ho = a.ho[qc];
-    if (threadIdx.x == 0) {
-        uint32_t lo = ownerOf(ho, 0u, H - 1, (unsigned long long)e0);
-        sm.range[0] = lo;
-        sm.range[1] = ownerOf(ho, lo, H - 1, (unsigned long long)(e1 - 1));
+    if (threadIdx.x < 64) {  // the chunk's first and last owners: warp 0 and warp 1 side by side
+        const unsigned long long key = threadIdx.x < 32 ? e0 : e1 - 1;
+        const uint32_t o = warpOwnerOf(ho, 0u, H - 1, key);
+        if ((threadIdx.x & 31u) == 0) sm.range[threadIdx.x >> 5] = o;
     }
     __syncthreads();
     const uint32_t lo = sm.range[0], hi = sm.range[1];
@@ -594,25 +598,44 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
                 tdGroups(a, S, G, qc, level, cur, a.bm[(level + 1) % 3], acc, fedges >= 65536, enq);
             }
             const uint32_t nt = warpMode ? 0u : (S + NT - 1) / NT;
+            // fewer tiles than half the blocks (a small queue, often of
+            // high-degree entries): every tile is split by edge range into
+            // parts of at least 8 NT edges, so its edges spread over the grid
+            // instead of running on nt blocks while the rest wait
+            uint32_t parts = 1;
+            if (nt && nt * 2 <= gridDim.x) {
+                const uint64_t perPart = (fedges > HE ? fedges - HE : 0) / nt / (8ull * NT);
+                const uint64_t cap = gridDim.x / nt;
+                parts = perPart < 1 ? 1u : (uint32_t)(perPart < cap ? perPart : cap);
+            }
+            const uint32_t nti = nt * parts;
             const uint64_t HC = (uint64_t)NT * 2;
             const bool pre = fedges >= 65536;
             const uint32_t nh = (uint32_t)((HE + HC - 1) / HC);
             uint32_t* bmNext = a.bm[(level + 1) % 3];
             // block b takes item b first; further items come from a ticket
+            // (none when the first items cover the level)
+            const bool oneRound = nti + nh <= gridDim.x;
             for (bool first = true;; first = false) {
-                if (tid == 0) sm.item = first ? blockIdx.x : gridDim.x + atomicAdd(&cur->work, 1u);
+                if (tid == 0)
+                    sm.item = first ? blockIdx.x : oneRound ? ~0u : gridDim.x + atomicAdd(&cur->work, 1u);
                 __syncthreads();
                 const uint32_t item = sm.item;
                 __syncthreads();
-                if (item >= nt + nh) break;
-                if (item < nt) {
+                if (item >= nti + nh) break;
+                if (item < nti) {
+                    const uint32_t tile = item / parts, part = item - tile * parts;
                     switch (strat) {
-                        case GB_STRAT_TD_EPT1: tdTile<NT, 1>(a, sm, item, S, qc, level, cur, bmNext, acc, pre, enq); break;
-                        case GB_STRAT_TD_EPT4: tdTile<NT, 4>(a, sm, item, S, qc, level, cur, bmNext, acc, pre, enq); break;
-                        default: tdTile<NT, 2>(a, sm, item, S, qc, level, cur, bmNext, acc, pre, enq); break;
+                        case GB_STRAT_TD_EPT1:
+                            tdTile<NT, 1>(a, sm, tile, S, qc, level, cur, bmNext, acc, pre, enq, part, parts);
+                            break;
+                        case GB_STRAT_TD_EPT4:
+                            tdTile<NT, 4>(a, sm, tile, S, qc, level, cur, bmNext, acc, pre, enq, part, parts);
+                            break;
+                        default: tdTile<NT, 2>(a, sm, tile, S, qc, level, cur, bmNext, acc, pre, enq, part, parts); break;
                     }
                 } else {
-                    const uint64_t e0 = (uint64_t)(item - nt) * HC;
+                    const uint64_t e0 = (uint64_t)(item - nti) * HC;
                     tdHubChunk<NT>(a, sm, e0, min(e0 + HC, HE), H, qc, level, cur, bmNext, acc, pre, enq);
                 }
             }

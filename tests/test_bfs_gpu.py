@@ -102,6 +102,26 @@ def test_persistent_strategy_mixes_exact(gb, oracle):
             assert np.array_equal(d, ref)
 
 
+def test_persistent_small_heavy_queue_split_exact(gb, oracle):
+    """A queue of fewer tiles than half the blocks, with many edges per tile,
+    is expanded in edge-range parts spread over the grid.  With the hub list
+    off (hub_min beyond every degree) every frontier goes through the tiles:
+    each edge-balanced strategy and the rule, on the full grid and on one
+    block per SM, must give the oracle's depths."""
+    g = gb.gen.rmat(16, 16, False, 1)
+    bfs = gb.GpuBfs(g)
+    for s in gb.pick_sources(g, 4, 7):
+        ref = oracle.bfs_serial(g, int(s))
+        for strat in ("td_ept1", "td_ept2", "td_ept4", None):
+            for grid in (0, 148):
+                kw = dict(hub_min=1 << 30, grid_blocks=grid)
+                if strat:
+                    kw["force_strategy"] = strat
+                d, tr = bfs.run("gpu_do_persistent", int(s), opts=gb.BfsOptions(**kw), trace=True)
+                assert np.array_equal(d, ref), (int(s), strat, grid)
+                assert sum(L["frontier"] for L in tr) == reached(ref)
+
+
 def test_hybrid_is_the_persistent_kernel(cases, gb, oracle):
     name, g, bfs, refs = cases[6]
     for src, ref in refs.items():
