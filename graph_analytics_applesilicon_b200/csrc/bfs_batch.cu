@@ -177,9 +177,11 @@ __device__ __forceinline__ void foldBits(const BArgs& a, uint64_t v, unsigned lo
 
 // Top-down push of one tile of NT active entries (edge-balanced, as the
 // single-source kernel): the entry's frontier mask minus the target's seen
-// mask is ORed into nx[target]; the first pusher records a candidate.
+// mask is ORed into nx[target]; the first pusher records a candidate.  The
+// block pushes part `part` of `parts` equal slices of the tile's edges.
 template <int NT, int EPT>
-__device__ void pushTile(const BArgs& a, BSmem<NT>& sm, uint32_t item, uint32_t S, uint32_t qc, BCounters* cur) {
+__device__ void pushTile(const BArgs& a, BSmem<NT>& sm, uint32_t item, uint32_t S, uint32_t qc, BCounters* cur,
+                         uint32_t part, uint32_t parts) {
     const uint32_t idx = item * NT + threadIdx.x;
     uint32_t st = 0, d = 0;
     unsigned long long f = 0;
@@ -195,7 +197,8 @@ __device__ void pushTile(const BArgs& a, BSmem<NT>& sm, uint32_t item, uint32_t 
     sm.f[threadIdx.x] = f;
     __syncthreads();
     const uint32_t cnt = min((uint32_t)NT, S - item * NT);
-    for (uint32_t base = 0; base < tot; base += NT * EPT) {
+    const uint32_t lo = (uint32_t)((uint64_t)tot * part / parts), hi = (uint32_t)((uint64_t)tot * (part + 1) / parts);
+    for (uint32_t base = lo; base < hi; base += NT * EPT) {
         uint32_t u[EPT];
         unsigned long long fu[EPT];
 #pragma unroll
@@ -203,7 +206,7 @@ __device__ void pushTile(const BArgs& a, BSmem<NT>& sm, uint32_t item, uint32_t 
             const uint32_t e = base + k * NT + threadIdx.x;
             u[k] = 0;
             fu[k] = 0;
-            if (e < tot) {
+            if (e < hi) {
                 const uint32_t o = ownerOf(sm.off, 0u, cnt - 1, e);
                 u[k] = a.col_idx[sm.st[o] + (e - sm.off[o])];
                 fu[k] = sm.f[o];
@@ -430,6 +433,16 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
             const uint64_t HE = hp & kHubMask;
             const uint32_t per = strat == GB_STRAT_TD_WARP ? NT / 32 : NT;
             const uint32_t nt = (S + per - 1) / per;
+            // fewer edge-balanced tiles than half the blocks: each is split by
+            // edge range into parts of at least 8 NT edges (as the
+            // single-source kernel)
+            uint32_t parts = 1;
+            if (strat != GB_STRAT_TD_WARP && nt && nt * 2 <= gridDim.x) {
+                const uint64_t perPart = (fedges > HE ? fedges - HE : 0) / nt / (8ull * NT);
+                const uint64_t cap = gridDim.x / nt;
+                parts = perPart < 1 ? 1u : (uint32_t)(perPart < cap ? perPart : cap);
+            }
+            const uint32_t nti = nt * parts;
             const uint64_t HC = (uint64_t)NT * 4;
             const uint32_t nh = (uint32_t)((HE + HC - 1) / HC);
             for (bool first = true;; first = false) {  // block b takes item b first
@@ -437,16 +450,17 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                 __syncthreads();
                 const uint32_t item = sm.item;
                 __syncthreads();
-                if (item >= nt + nh) break;
-                if (item < nt) {
+                if (item >= nti + nh) break;
+                if (item < nti) {
+                    const uint32_t tile = item / parts, part = item - tile * parts;
                     switch (strat) {
-                        case GB_STRAT_TD_EPT1: pushTile<NT, 1>(a, sm, item, S, qc, cur); break;
-                        case GB_STRAT_TD_EPT4: pushTile<NT, 4>(a, sm, item, S, qc, cur); break;
+                        case GB_STRAT_TD_EPT1: pushTile<NT, 1>(a, sm, tile, S, qc, cur, part, parts); break;
+                        case GB_STRAT_TD_EPT4: pushTile<NT, 4>(a, sm, tile, S, qc, cur, part, parts); break;
                         case GB_STRAT_TD_WARP: pushWarpItem<NT>(a, item, S, qc, cur); break;
-                        default: pushTile<NT, 2>(a, sm, item, S, qc, cur); break;
+                        default: pushTile<NT, 2>(a, sm, tile, S, qc, cur, part, parts); break;
                     }
                 } else {
-                    const uint64_t e0 = (uint64_t)(item - nt) * HC;
+                    const uint64_t e0 = (uint64_t)(item - nti) * HC;
                     pushHubChunk<NT>(a, sm, e0, min(e0 + HC, HE), H, qc, cur);
                 }
             }

@@ -51,6 +51,21 @@ def test_batch_larger_graphs(gb, oracle):
             check_batch(gb, oracle, g, bfs, srcs, opts)
 
 
+def test_batch_small_heavy_queue_split_exact(gb, oracle):
+    """Few edge-balanced tiles with many edges each (hub list off) are pushed
+    in edge-range parts over the grid: every edge-balanced strategy, on the
+    full grid and on small ones, must give the oracle's depths for every
+    source of the batch."""
+    g = gb.gen.rmat(16, 16, False, 1)
+    bfs = gb.GpuBfs(g)
+    for k, seed in ((64, 9), (5, 3)):
+        srcs = gb.pick_sources(g, k, seed)
+        for strat in ("td_ept1", "td_ept2", "td_ept4"):
+            for grid in (0, 148, 16):
+                opts = gb.BfsOptions(force_strategy=strat, hub_min=1 << 30, grid_blocks=grid)
+                check_batch(gb, oracle, g, bfs, srcs, opts)
+
+
 def test_batch_learned_selector_exact(gb, oracle):
     g = gb.gen.rmat(15, 16, False, 8)
     bfs = gb.GpuBfs(g)
