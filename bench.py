@@ -32,6 +32,7 @@ its own GPU; value = all ranks' edges / max rank time.
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -169,33 +170,78 @@ def check_depths(g, dist, src):
     return bool(has_parent[reached].all())
 
 
-def cpu_baseline(g, srcs, budget_s=15.0):
-    """The reference's cpu_do on all host threads (oracle/_ref), bounded sample."""
+def _oracle():
+    """The oracle package (test infrastructure): the reference's own CPU code
+    built from its sources (oracle/_ref) and the C restatement.  bench.py
+    uses it only as the checker, as the timed CPU baseline and in the
+    reference arm -- never on the measured path."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as O
-    if O.ref() is not None:
-        rg = O.RefGraph.of(O.HostGraph(g.n, g.m, g.flags, g.row_ptr, g.col_idx))
-        cores = int(O.ref().gref_max_threads())
-        run = lambda s: rg.bfs_do(int(s), 15.0, 18.0, threads=0, trace=False)[0]
-        kind = "reference"
-    else:
-        hg = O.HostGraph(g.n, g.m, g.flags, g.row_ptr, g.col_idx)
-        cores = 1
-        run = lambda s: O.bfs_do(hg, int(s))[0]
-        kind = "port"
-    edges, secs, used = 0, 0.0, 0
-    run(srcs[0])  # warm-up
-    t_start = time.time()
-    for s in srcs:
+    return O
+
+
+def depth_hash(d) -> bytes:
+    return hashlib.blake2b(np.ascontiguousarray(d).view(np.uint8), digest_size=16).digest()
+
+
+class ReferenceBfs:
+    """The reference's cpu_do (src/cpu/bfs_cpu.cpp:227-283; alpha 15, beta 18,
+    all host threads) on a host copy of the graph, from oracle/_ref; the
+    oracle's one-thread restatement when the reference build is absent."""
+
+    def __init__(self, n, m, flags, row_ptr, col_idx, ref_graph=None):
+        O = _oracle()
+        self.deg = np.diff(row_ptr.astype(np.int64))
+        if ref_graph is not None or O.ref() is not None:
+            self.rg = ref_graph if ref_graph is not None else O.RefGraph.of(
+                O.HostGraph(n, m, flags, row_ptr, col_idx))
+            self.cores = int(O.ref().gref_max_threads())
+            self.kind = "reference"
+            self._run = lambda s: self.rg.bfs_do(int(s), 15.0, 18.0, threads=0, trace=False)[0]
+        else:
+            hg = O.HostGraph(n, m, flags, row_ptr, col_idx)
+            self.cores, self.kind = 1, "port"
+            self._run = lambda s: O.bfs_do(hg, int(s))[0]
+
+    def run(self, s):
+        """(depths, seconds)"""
         t0 = time.perf_counter()
-        d = run(s)
-        secs += time.perf_counter() - t0
-        edges += component_edges(g, d)
-        used += 1
-        if time.time() - t_start > budget_s:
-            break
-    return {"value": edges / secs / 1e9, "unit": "GTEPS", "cores": cores, "kind": kind,
-            "sample": f"cpu_do alpha=15 beta=18 from {used} of the {len(srcs)} sources, {secs:.1f}s"}
+        d = self._run(s)
+        return d, time.perf_counter() - t0
+
+    def comp_edges(self, d) -> int:
+        return int(self.deg[d != 0xFFFFFFFF].sum()) // 2
+
+
+def check_against_reference(g, sources, own, hashes, ref=None, timed=64):
+    """Every source's GPU depths against the reference's cpu_do, bit for bit.
+    own: {source index: GPU depth array} compared element-wise; hashes: {source
+    index: 16-byte digest of the GPU depths} for depths held elsewhere (other
+    ranks).  Returns (ok, first mismatch, per-source component edges from the
+    REFERENCE depths -- the TEPS denominators of src/bench/main.cpp:329-332 --
+    and the cpu_baseline record of the first `timed` sources)."""
+    ref = ref or ReferenceBfs(g.n, g.m, g.flags, g.row_ptr, g.col_idx)
+    ref.run(sources[0])  # warm-up
+    comp, secs, edges, bad = [], 0.0, 0, None
+    for i, s in enumerate(sources):
+        d, dt = ref.run(s)
+        c = ref.comp_edges(d)
+        comp.append(c)
+        if i < timed:
+            secs += dt
+            edges += c
+        if i in own:
+            same = np.array_equal(own[i], d)
+        elif i in hashes:
+            same = hashes[i] == depth_hash(d)
+        else:
+            same = None
+        if same is False and bad is None:
+            bad = {"source_index": i, "source": int(s)}
+    used = min(timed, len(sources))
+    cpu = {"value": edges / secs / 1e9, "unit": "GTEPS", "cores": ref.cores, "kind": ref.kind,
+           "sample": f"cpu_do alpha=15 beta=18 on all {used} sources of rank 0, {secs:.1f}s"}
+    return bad is None, bad, comp, cpu
 
 
 def max_over_ranks(vals, world):
@@ -213,15 +259,19 @@ def max_over_ranks(vals, world):
     return t.tolist()
 
 
-def measured_traffic(kernel, workload):
-    """DRAM bytes (read + write) per launch of `kernel` on `workload`, as measured by ncu
-    and recorded in profiles/roofline_traffic.txt (None if not recorded)."""
+def measured_traffic(kernel, workload, grid_blocks):
+    """DRAM bytes (read + write) per launch of `kernel` on `workload` at a grid of
+    `grid_blocks` blocks (None: any), as measured by ncu and recorded in
+    profiles/roofline_traffic.txt; None when no capture of that launch shape
+    is recorded."""
     try:
         with open(os.path.join(ROOT, "profiles", "roofline_traffic.txt")) as f:
             for line in f:
                 parts = line.split()
-                if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and parts[1] == workload:
-                    return int(parts[2])
+                if line.startswith("#") or len(parts) < 4 or parts[0] != kernel or parts[1] != workload:
+                    continue
+                if grid_blocks is None or parts[2] in ("*", str(grid_blocks)):
+                    return int(parts[3])
     except OSError:
         pass
     return None
@@ -240,26 +290,98 @@ def init_dist(args):
     return world, rank, local
 
 
+def secondary_workloads(args, local):
+    """The other benchmark configurations, measured in the same process after
+    the headline (1 GPU): Chung-Lu 20-iteration PageRank and 64-source batch,
+    web PageRank to tol 1e-6, road-grid persistent vs plain BFS.  Each is
+    checked against the reference's own CPU code; the summary of each line is
+    kept (the full lines come from --workload <name>)."""
+    import argparse as _a
+    import graph_analytics_applesilicon_b200 as G
+    sub = _a.Namespace(**vars(args))
+    sub.steps, sub.warmup = 5, 3
+    out = {}
+
+    def keep(line, keys):
+        return {k: line.get(k) for k in keys if k in line}
+
+    common = ("value", "unit", "ms_per_step", "higher_is_better", "config", "e2e", "roofline", "clocks",
+              "validated", "validated_sources", "cpu_baseline", "compare")
+    t = time.time()
+    sub.workload = "road_bfs"
+    out["road_bfs"] = keep(bfs_config_workload(sub, 1, 0, local), common)
+    sub.workload = "web_pr_tol"
+    out["web_pr_tol"] = keep(pagerank_tol_workload(sub, 1, 0, local),
+                             ("value", "unit", "config", "e2e", "results", "gs_accuracy_ok", "reference_check",
+                              "validated"))
+    cl = G.gen.chung_lu(3070000, 2.2, 76.0, 307)
+    sub.workload = "chunglu_pr20"
+    sub.n = cl.n
+    out["chunglu_pr20"] = keep(pagerank_workload(sub, 1, 0, local, g=cl),
+                               common + ("accuracy", "reference_check"))
+    sub.workload = "chunglu_bfs64"
+    out["chunglu_bfs64"] = keep(bfs_config_workload(sub, 1, 0, local, g=cl), common)
+    log(f"secondary workloads: {time.time() - t:.1f}s")
+    return out
+
+
+def headline_config(n, m, world, per_rank):
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": WORKLOAD, "graph": "rmat scale 22, 8.5*2^22 drawn edges (seed 22), ids permuted (seed 1)",
+            "n": n, "m": m, "sources_per_rank": per_rank, "sources_total": per_rank * world,
+            "parallelism": f"sources split over {world} GPU(s)" if world > 1 else "1 GPU",
+            "l2": "inputs larger than L2 (CSR 293 MB)"}
+
+
 def reference_arm(args, world, rank):
+    """The reference's own CPU BFS (cpu_do, alpha 15 / beta 18, all host
+    threads) on the benchmark graph, everything from oracle/_ref: the graph is
+    built by the reference's fromEdgeList, reorder "random" and permute from
+    the restated quadrant draw, sources by the oracle's pickSources.  This
+    library is not imported.  One step = cpu_do over 64 sources (at N > 1 a
+    window of 64 of the 64*N sources, rotating per step)."""
     if rank != 0:
         return
-    import graph_analytics_applesilicon_b200 as G
-    g, srcs = build_graph(G, gpu_prep=False)
-    per_step = 20.0 / max(1, args.steps + args.warmup)
-    for _ in range(args.warmup):
-        cpu_baseline(g, srcs, per_step)
-    vals = []
-    t0 = time.time()
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(g, srcs, per_step))
-    wall = time.time() - t0
-    v = statistics.median([x["value"] for x in vals])
+    O = _oracle()
+    t = time.time()
+    if O.ref() is not None:
+        rg = O.ref_rmat_graph(SCALE, EDGES_DRAWN, GEN_SEED, PERM_SEED)
+        hg = rg.host()
+    else:  # the oracle's restatement of the same construction
+        rg = None
+        hg = O.permute(O.gen("rmat_edges", SCALE, EDGES_DRAWN, 0, GEN_SEED), O.random_perm(1 << SCALE, PERM_SEED))
+    srcs_all = O.pick_sources(hg, args.sources * world, 1)
+    log(f"reference graph n={hg.n} m={hg.m} built in {time.time() - t:.1f}s")
+    ref = ReferenceBfs(hg.n, hg.m, hg.flags, hg.row_ptr, hg.col_idx, ref_graph=rg)
+    comp = {}
+
+    def step(i):
+        k = len(srcs_all)
+        window = [srcs_all[(i * args.sources + j) % k] for j in range(min(args.sources, k))]
+        secs, edges = 0.0, 0
+        for s in window:
+            d, dt = ref.run(s)
+            if int(s) not in comp:
+                comp[int(s)] = ref.comp_edges(d)
+            secs += dt
+            edges += comp[int(s)]
+        return secs, edges
+
+    for i in range(args.warmup):
+        step(i)
+    secs = edges = 0
+    for i in range(args.steps):
+        a, b = step(args.warmup + i)
+        secs += a
+        edges += b
+    v = edges / secs / 1e9
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GTEPS", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / max(1, args.steps) * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / max(1, args.steps) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "n": g.n, "m": g.m, "sources": len(srcs)},
-            "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": vals[0]["cores"], "kind": vals[0]["kind"],
-                             "sample": vals[0]["sample"]},
+            "data": "synthetic", "config": headline_config(hg.n, hg.m, world, args.sources),
+            "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": ref.cores, "kind": ref.kind,
+                             "sample": f"cpu_do alpha=15 beta=18, {args.sources} sources per step, "
+                                       f"{args.steps} steps, {secs:.1f}s"},
             "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -273,26 +395,28 @@ def _timed(fn, reps=1):
     return best * 1e3
 
 
-def bfs_config_workload(args, world, rank, local):
+def bfs_config_workload(args, world, rank, local, g=None):
     """road_bfs: 1400 x 1400 road-shaped grid (4% of edges dropped, 0.5% diagonal
     links, seed 1400; ~1.96M vertices, diameter > 1400 levels); 8 sources,
     single-source persistent BFS vs the per-level plain gpu_do, plus the
     64-source batch in one launch vs 64 plain runs.
     chunglu_bfs64: Chung-Lu graph (3.07M vertices, gamma 2.2, mean degree 76,
     seed 307); one 64-source batch in one launch with the learned batched
-    selector and autotuned hub cut / block size, vs 64 plain gpu_do runs."""
+    selector and autotuned hub cut / block size, vs 64 plain gpu_do runs.
+    Every batch row is checked against the reference's cpu_do, and the TEPS
+    denominators come from the reference's depths."""
     import torch
     import graph_analytics_applesilicon_b200 as G
     torch.cuda.set_device(local)
     t = time.time()
     road = args.workload == "road_bfs"
-    g = G.gen.road(1400, 1400, 0.04, 0.005, 1400) if road else G.gen.chung_lu(3070000, 2.2, 76.0, 307)
+    if g is None:
+        g = G.gen.road(1400, 1400, 0.04, 0.005, 1400) if road else G.gen.chung_lu(3070000, 2.2, 76.0, 307)
     log(f"{args.workload}: n={g.n} m={g.m} built in {time.time() - t:.1f}s")
     srcs64 = G.pick_sources_gpu(g, 64, 1)
     bfs = G.GpuBfs(g)
     if args.adjacency == "hub-first":
         bfs.hub_first()  # device layout only: same depths, earlier bottom-up exits
-    comp = {int(s): component_edges(g, bfs.run("gpu_do_persistent", int(s))) for s in srcs64}
     sel1, sel2 = G.default_selector_params("single"), G.default_selector_params("batch")
     if sel1 is not None:
         bfs.set_selector(sel1, 0)
@@ -309,12 +433,8 @@ def bfs_config_workload(args, world, rank, local):
         bfs.run_batch(srcs64, opts=ob_)
         batch_cands[sel] = (bfs.lastGpuMs(), ob_)
     ob = min(batch_cands.values(), key=lambda x: x[0])[1]
-    # exactness of the batch against single-source runs (size-independent)
     d64 = bfs.run_batch(srcs64, opts=ob)
     batch_levels = bfs.lastLevels()
-    for i in (0, 17, 63):
-        assert np.array_equal(d64[i], bfs.run("gpu_do_persistent", int(srcs64[i]))), "batch != single"
-    valid = check_depths(g, d64[0], int(srcs64[0]))
     for _ in range(args.warmup):
         bfs.run_batch(srcs64, opts=ob)
     with ClockSampler(local) as clocks:
@@ -338,16 +458,27 @@ def bfs_config_workload(args, world, rank, local):
     plain_e2e = [_timed(lambda: pb.run("gpu_do", int(s))) for s in plain[:2]]
     if pb is not bfs:
         pb.close()
+    # the single-source forms on a few sources, for the check below
+    singles = {i: bfs.run("gpu_do_persistent", int(srcs64[i]), opts=o1) for i in (0, 17, 63)}
+    bfs.close()
     batch_t, e2e = max_over_ranks([statistics.median(batch_ms), e2e], world)
     if rank != 0:
-        return
-    e64 = sum(comp.values())
-    single_gteps = sum(comp[int(s)] for s in single) / (sum(single_ms) * 1e-3) / 1e9
-    plain_gteps = sum(comp[int(s)] for s in plain) / (sum(plain_ms) * 1e-3) / 1e9
+        return None
+    # every batch row (the e2e call's host output) and the single-source runs
+    # against the reference's cpu_do; TEPS denominators from the reference
+    valid, bad, comp, cpu = check_against_reference(g, list(srcs64), {i: pinned[i] for i in range(64)}, {})
+    valid = valid and all(np.array_equal(d64[i], pinned[i]) and np.array_equal(d, pinned[i])
+                          for i, d in singles.items())
+    cidx = {int(s): c for s, c in zip(srcs64, comp)}
+    e64 = sum(comp)
+    single_gteps = sum(cidx[int(s)] for s in single) / (sum(single_ms) * 1e-3) / 1e9
+    plain_gteps = sum(cidx[int(s)] for s in plain) / (sum(plain_ms) * 1e-3) / 1e9
     value = world * e64 / (batch_t * 1e-3) / 1e9  # every rank runs its own batch (replicas)
     peak, peak_kind = peaks()
     bytes_per_trav = 4 * (g.n + 1) + 4 * g.m + 4 * g.n
     achieved = 64 * bytes_per_trav / (batch_t * 1e-3) / 1e9
+    traffic = measured_traffic("batchBfsKernel", args.workload, ob.grid_blocks)
+    dram = traffic / (batch_t * 1e-3) / 1e9 if traffic else None
     line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": batch_t, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64 masks / u32 depths", "data": "synthetic",
@@ -362,10 +493,12 @@ def bfs_config_workload(args, world, rank, local):
                     "result_bytes_per_step": 4 * 64 * g.n},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_source": peak_kind, "kernel": "batchBfsKernel",
+                         "traffic": traffic, "peak_source": peak_kind, "kernel": "batchBfsKernel",
                          "bytes_per_launch": 64 * bytes_per_trav, "mean_launch_ms": batch_t,
-                         "note": "graph-pass equivalents: 64 traversals per launch"},
-            "clocks": clocks.summary(), "validated": bool(valid),
+                         "note": "graph-pass equivalents: 64 traversals per launch",
+                         "dram_achieved": dram, "dram_frac": dram / peak if dram else None},
+            "clocks": clocks.summary(), "validated": bool(valid), "validated_sources": 64 if valid else 0,
+            "cpu_baseline": cpu,
             "compare": {"batch64_one_launch_gteps": value,
                         "single_source_persistent_gteps": single_gteps,
                         "single_selector": o1.selector,
@@ -375,7 +508,9 @@ def bfs_config_workload(args, world, rank, local):
                         "persistent_ms_per_source": statistics.mean(single_ms),
                         "speedup_persistent_vs_plain": statistics.mean(plain_ms) / statistics.mean(single_ms),
                         "speedup_batch_vs_64_plain": 64 * statistics.mean(plain_ms) / batch_t}}
-    print(json.dumps(line), flush=True)
+    if bad is not None:
+        line["validation_failure"] = bad
+    return line
 
 
 def edge_text(u, v) -> bytes:
@@ -459,7 +594,7 @@ def snap_convert_workload(args, world, rank, local):
         os.unlink(f)
     os.rmdir(tmp)
     if rank != 0:
-        return
+        return None
     line = {"metric": "SNAP text -> CSR .bin conversion (gconvert)", "value": value, "unit": "M lines/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 text / u32 ids",
@@ -468,15 +603,17 @@ def snap_convert_workload(args, world, rank, local):
             "e2e": {"value": value, "unit": "M lines/s", "h2d_bytes_per_step": text_bytes,
                     "d2h_bytes_per_step": 4 * (conv.n + 1 + conv.m)},
             "roofline": None, "cpu_baseline": cpu, "validated": ok, "stats": st}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def pagerank_tol_workload(args, world, rank, local):
     """Web-shaped directed graph (875,000 vertices, geometric out-degree mean
     5.8 -> ~15% dangling, Zipf s=2.1 in-degree, seed 875): PageRank to tol 1e-6,
     Jacobi (degree-adaptive pull) vs in-place Gauss-Seidel (pair deferral K=2),
-    FP32 against the FP64 GPU oracle.  value: ms to tol of the faster method
-    that meets its accuracy rule."""
+    FP32 against the FP64 GPU oracle and against the reference's own
+    pagerankSerial with checkRanks (Jacobi forms) or gsNoWorseThanJacobi
+    (Gauss-Seidel), as gbench --validate does (src/bench/main.cpp:474-495).
+    value: ms to tol of the faster method that meets its accuracy rule."""
     import torch
     import graph_analytics_applesilicon_b200 as G
     torch.cuda.set_device(local)
@@ -489,7 +626,7 @@ def pagerank_tol_workload(args, world, rank, local):
     ref_jac = pr.ranks_f64()
     pr.run("gpu_pull_f64", G.PrOptions(tol=1e-12, iters=2000))
     conv = pr.ranks_f64()
-    res = {}
+    res, final = {}, {}
     for v in ("gpu_pull_adaptive", "gpu_pull_vector", "gpu_pull_gs"):
         for _ in range(args.warmup):
             pr.run(v, o)
@@ -498,6 +635,7 @@ def pagerank_tol_workload(args, world, rank, local):
             r = pr.run(v, o)
             ts.append(r.gpu_ms)
         got = pr.ranks().astype(np.float64)
+        final[v] = pr.ranks()
         res[v] = {"ms_to_tol": statistics.median(ts), "iters": r.iters, "last_delta": r.last_delta,
                   "l1_vs_fp64_same_method": float(np.abs(got - ref_jac).sum()),
                   "l1_vs_converged": float(np.abs(got - conv).sum()), "sum": float(got.sum())}
@@ -507,28 +645,74 @@ def pagerank_tol_workload(args, world, rank, local):
         else "gpu_pull_adaptive"
     res[best]["ms_to_tol"] = max_over_ranks([res[best]["ms_to_tol"]], world)[0]  # the slowest replica
     if rank != 0:
-        return
+        pr.close()
+        return None
     out = torch.empty(g.n, dtype=torch.float32, pin_memory=True).numpy()
     e2e = _timed(lambda: (pr.run(best, o), G.check(G.lib().gb_pr_ranks(pr._h, out))), 3)
+    pr.close()
+    reference = pagerank_reference_check(gin, g.degrees(), final, 1000, 1e-6)
+    valid = reference.get("ok") if reference else None
     line = {"metric": METRIC, "value": res[best]["ms_to_tol"], "unit": "ms to tol 1e-6", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[best]["ms_to_tol"],
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 residual)",
             "data": "synthetic", "config": {"workload": "web_pr_tol", "n": g.n, "m": g.m, "method": best},
             "e2e": {"value": e2e, "unit": "ms to tol 1e-6", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4 * g.n},
-            "gpu_launches": None, "results": res, "fp64_jacobi_vs_converged_l1": jac_l1, "gs_accuracy_ok": gs_ok}
-    print(json.dumps(line), flush=True)
+            "gpu_launches": None, "results": res, "fp64_jacobi_vs_converged_l1": jac_l1, "gs_accuracy_ok": gs_ok,
+            "reference_check": reference, "validated": valid}
+    return line
 
 
-def pagerank_workload(args, world, rank, local):
+def pagerank_reference_check(gin, outdeg, ranks: dict, iters: int, tol: float, serial=True):
+    """The reference's own PageRank (oracle/_ref: pagerankSerial, or
+    pagerankOmp with all host threads for the 234M-edge graph -- the same
+    per-vertex double sums in parallel) on the full graph, and its checkRanks
+    (L1 < 1e-4, top-1000 relative error < 1e-3, |sum - 1| < 1e-4) of every
+    FP32 result in `ranks`.  Gauss-Seidel results are held to the reference's
+    gsNoWorseThanJacobi against the converged (tol 1e-10) ranks, as gbench
+    --validate does.  None when the reference build is absent."""
+    O = _oracle()
+    if O.ref() is None:
+        return None
+    rg = O.RefGraph.of(O.HostGraph(gin.n, gin.m, gin.flags, gin.row_ptr, gin.col_idx))
+    threads = -1 if serial else 0
+    t0 = time.perf_counter()
+    ref, it, _ = rg.pagerank(outdeg, iters, tol, threads=threads)
+    ref_s = time.perf_counter() - t0
+    out = {"reference": ("pagerankSerial" if serial else "pagerankOmp (all threads)") + f", {it} iterations",
+           "reference_s": ref_s, "checks": {}}
+    ok = True
+    conv = jac = None
+    for name, r in ranks.items():
+        c = O.ref_check_ranks(ref, r)
+        rec = {"l1": c.l1, "max_rel_top1000": c.max_rel_top, "sum": c.sum}
+        if name == "gpu_pull_gs":
+            if conv is None:
+                conv, _, _ = rg.pagerank(outdeg, 1000, 1e-10, threads=threads)
+                jac = O.check_ranks(conv, ref)  # the Jacobi reference's own distance from convergence
+            cg = O.ref_check_ranks(conv, r)
+            rec["vs_converged"] = {"l1": cg.l1, "max_rel_top1000": cg.max_rel_top, "sum": cg.sum}
+            rec["ok"] = O.gs_no_worse(cg, jac)
+        else:
+            rec["ok"] = c.ok()
+        ok = ok and rec["ok"]
+        out["checks"][name] = rec
+    out["ok"] = ok
+    return out
+
+
+def pagerank_workload(args, world, rank, local, g=None):
     """Chung-Lu graph (3.07M vertices, gamma 2.2, mean degree 76, seed 307, ids
     permuted): 20 fixed Jacobi iterations of the degree-adaptive pull in FP32,
     one step = one 20-iteration run (a CUDA-graph replay), ms per iteration.
-    Checked against the double-precision GPU pull at L1 < 1e-4."""
+    Checked against the double-precision GPU pull at L1 < 1e-4 and against the
+    reference's own pagerankOmp (all host threads, 20 iterations) with its
+    checkRanks; that run is also the CPU baseline."""
     import torch
     import graph_analytics_applesilicon_b200 as G
     torch.cuda.set_device(local)
     t = time.time()
-    g = G.gen.chung_lu(args.n, 2.2, 76.0, 307)
+    if g is None:
+        g = G.gen.chung_lu(args.n, 2.2, 76.0, 307)
     log(f"chung-lu n={g.n} m={g.m} built in {time.time() - t:.1f}s")
     pr = G.GpuPageRank(g.n, g, g, g.degrees())  # undirected: out-CSR = in-CSR
     o = pr.autotune(G.PrOptions(iters=20))  # degree-class cut points and block size
@@ -561,31 +745,27 @@ def pagerank_workload(args, world, rank, local):
             G.check(G.lib().gb_pr_ranks(pr._h, out))
             e2e.append((time.perf_counter() - t0) * 1e3)
     total, e2e_sum = max_over_ranks([total, sum(e2e)], world)
+    final = pr.ranks()
     compare = {}
     for v in ("gpu_pull_vector", "gpu_pull_scalar", "gpu_push"):
         rr = [pr.run(v, o).gpu_ms for _ in range(2)]
         compare[v + "_ms_per_iter"] = min(rr) / 20
+    pr.close()
     if rank != 0:
-        return
+        return None
     ms_iter = total / args.steps / 20
     peak, peak_kind = peaks()
     bytes_sweep = 4 * (g.n + 1) + 8 * g.m + 4 * g.n
     kernel_ms = statistics.mean(gpu) / 20
     achieved = bytes_sweep / (kernel_ms * 1e-3) / 1e9
-    cpu = None
-    if not args.no_cpu_baseline and world == 1:
-        try:
-            sys.path.insert(0, os.path.join(ROOT, "oracle"))
-            import oracle_py as O
-            if O.ref() is not None:
-                rg = O.RefGraph.of(O.HostGraph(g.n, g.m, g.flags, g.row_ptr, g.col_idx))
-                t0 = time.perf_counter()
-                rg.pagerank(g.degrees(), 2, 0.0, threads=0)
-                sec = time.perf_counter() - t0
-                cpu = {"value": sec * 1e3 / 2, "unit": "ms/iter", "cores": int(O.ref().gref_max_threads()),
-                       "kind": "reference", "sample": "cpu_omp (dynamic,256), 2 iterations on the full graph"}
-        except Exception as e:
-            cpu = {"value": None, "error": str(e)[:200]}
+    cpu, reference = None, None
+    if world == 1:
+        reference = pagerank_reference_check(g, g.degrees(), {"gpu_pull_adaptive": final}, 20, 0.0, serial=False)
+        if reference is not None and not args.no_cpu_baseline:
+            O = _oracle()
+            cpu = {"value": reference["reference_s"] * 1e3 / 20, "unit": "ms/iter",
+                   "cores": int(O.ref().gref_max_threads()), "kind": "reference",
+                   "sample": "cpu_omp (dynamic,256), 20 iterations on the full graph"}
     line = {"metric": METRIC, "value": ms_iter, "unit": "ms/iter", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total / args.steps, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -596,54 +776,55 @@ def pagerank_workload(args, world, rank, local):
                     "d2h_bytes_per_step": 4 * g.n},
             "gpu_launches": 21 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": measured_traffic("prPullKernel<2>", "chunglu_pr20") if args.n == 3070000 else None,
+                         "traffic": (measured_traffic("prPullKernel<2>", "chunglu_pr20", None)
+                                     if args.n == 3070000 else None),
                          "peak_source": peak_kind, "kernel": "prPullKernel<2,false>",
                          "bytes_per_launch": bytes_sweep, "mean_launch_ms": kernel_ms},
             "cpu_baseline": cpu, "clocks": clocks.summary(),
-            "accuracy": {"l1_vs_fp64_gpu": l1, "ok": l1 < 1e-4}, "compare": compare}
-    print(json.dumps(line), flush=True)
+            "accuracy": {"l1_vs_fp64_gpu": l1, "ok": l1 < 1e-4}, "reference_check": reference,
+            "validated": (l1 < 1e-4) and (reference is None or reference["ok"]), "compare": compare}
+    return line
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-compare", action="store_true", help="skip the plain/rule comparison runs")
-    ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (smaller: profiling cases)")
-    ap.add_argument("--sources", type=int, default=NSRC)
-    ap.add_argument("--workload", default=WORKLOAD,
-                    choices=[WORKLOAD, "chunglu_pr20", "road_bfs", "chunglu_bfs64", "web_pr_tol", "snap_convert"],
-                    help="rmat22_bfs64 (default, the headline); chunglu_pr20, road_bfs, chunglu_bfs64, web_pr_tol, "
-                         "snap_convert")
-    ap.add_argument("--n", type=int, default=3070000, help="chunglu_pr20: vertices")
-    ap.add_argument("--adjacency", default="hub-first", choices=["hub-first", "natural"],
-                    help="BFS device adjacency layout (hub-first: lists by descending neighbour degree; same depths)")
-    args = ap.parse_args()
-    world, rank, local = init_dist(args)
-    if args.impl == "reference":
-        reference_arm(args, world, rank)
-        return
-    args.warmup = max(3, args.warmup)
-    if args.workload == "chunglu_pr20":
-        pagerank_workload(args, world, rank, local)
-        return
-    if args.workload in ("road_bfs", "chunglu_bfs64"):
-        bfs_config_workload(args, world, rank, local)
-        return
-    if args.workload == "web_pr_tol":
-        pagerank_tol_workload(args, world, rank, local)
-        return
-    if args.workload == "snap_convert":
-        snap_convert_workload(args, world, rank, local)
-        return
+def gather_rows(rows: np.ndarray, world: int) -> list:
+    """All ranks' int64 rows (same shape on every rank), in rank order: the
+    per-source results of a split batch meet on rank 0 (NCCL on a GPU run,
+    gloo in the CPU tests)."""
+    if world <= 1:
+        return [rows]
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.from_numpy(np.ascontiguousarray(rows, np.int64)).to(dev)
+    out = [torch.empty_like(t) for _ in range(world)]
+    dist.all_gather(out, t)
+    return [o.cpu().numpy() for o in out]
 
+
+def source_rows(depths: np.ndarray, deg: np.ndarray) -> np.ndarray:
+    """Per source: (GPU component edges, depth digest as two int64 words)."""
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(8) as ex:
+        digests = list(ex.map(lambda d: depth_hash(d), depths))
+    rows = np.zeros((len(depths), 3), np.int64)
+    for i, d in enumerate(depths):
+        rows[i, 0] = int(deg[d != 0xFFFFFFFF].sum()) // 2
+        rows[i, 1:] = np.frombuffer(digests[i], np.int64)
+    return rows
+
+
+def split_sources(srcs_all, world, rank, per_rank):
+    """Rank k runs sources [k*per_rank, (k+1)*per_rank) of the 64*N picked
+    sources: no source runs twice and rank 0 keeps the single-GPU set."""
+    return srcs_all[rank * per_rank:(rank + 1) * per_rank]
+
+
+def headline_workload(args, world, rank, local):
     import torch
     import graph_analytics_applesilicon_b200 as G
     torch.cuda.set_device(local)
-    g, srcs = build_graph(G, args.scale, args.sources)
+    g, srcs_all = build_graph(G, args.scale, args.sources * world)
+    srcs = split_sources(srcs_all, world, rank, args.sources)
     bfs = G.GpuBfs(g)
     if args.adjacency == "hub-first":
         bfs.hub_first()  # device layout only: same depths, earlier bottom-up exits
@@ -663,22 +844,20 @@ def main():
             bfs.run("gpu_do_persistent", int(s_), opts=o)
             t_ += bfs.lastGpuMs()
         cands[name] = (t_, o)
-    selector = min(cands, key=lambda k: cands[k][0])
+    if world > 1:  # every rank must run the same selector and options
+        import torch.distributed as dist
+        votes = torch.tensor([cands[k][0] for k in sorted(cands)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(votes, op=dist.ReduceOp.SUM)
+        selector = sorted(cands)[int(torch.argmin(votes))]
+    else:
+        selector = min(cands, key=lambda k: cands[k][0])
     opts = cands[selector][1]
     stream = torch.cuda.ExternalStream(G.lib().gb_bfs_stream(bfs._h))
 
-    # exactness of one result (size-independent check) and TEPS denominators
-    comp = []
-    d0 = None
-    max_levels = 0
-    for i, s in enumerate(srcs):
-        d = bfs.run("gpu_do_persistent", int(s), opts=opts)
+    max_levels = 0  # sets the packed depth width on the PCIe wire
+    for s in srcs:
+        bfs.run("gpu_do_persistent", int(s), opts=opts)
         max_levels = max(max_levels, bfs.lastLevels())
-        comp.append(component_edges(g, d))
-        if i == 0:
-            d0 = d.copy()
-    valid = check_depths(g, d0, int(srcs[0]))
-    edges_per_step = sum(comp)
 
     def device_step(variant="gpu_do_persistent", o=opts, h=bfs):
         # one gb_bfs_run_many call: the persistent traversals follow one
@@ -724,11 +903,12 @@ def main():
         barrier()
         e2e_distinct_ms = [e2e_step(distinct, g.n) for _ in range(args.steps)]
         barrier()
-    total_ms = sum(step_ms)
-    e2e_total = sum(e2e_ms)
-    total_ms, e2e_total, e2e_distinct_total = max_over_ranks([total_ms, e2e_total, sum(e2e_distinct_ms)], world)
-    distinct_ok = all(np.array_equal(distinct[i], bfs.run("gpu_do_persistent", int(s), opts=opts))
-                      for i, s in enumerate(srcs[:4]))
+    total_ms, e2e_total, e2e_distinct_total = max_over_ranks([sum(step_ms), sum(e2e_ms), sum(e2e_distinct_ms)],
+                                                             world)
+    # the last timed step left every source's depths in `distinct` (the output
+    # of the public call): their digests meet on rank 0 for the reference check
+    deg = np.diff(g.row_ptr.astype(np.int64))
+    rows = gather_rows(source_rows(distinct, deg), world)
 
     # comparison forms on the same sources (not part of the timed region)
     plain_ms = rule_ms = learned_ms = float("nan")
@@ -747,6 +927,21 @@ def main():
         if "learned" in cands:
             device_step("gpu_do_persistent", cands["learned"][1])
             learned_ms = device_step("gpu_do_persistent", cands["learned"][1])[0]
+    if rank != 0:
+        return None
+
+    # every depth array of every rank against the reference's cpu_do, bit for
+    # bit; the TEPS denominators come from the reference's depths
+    own = {i: distinct[i] for i in range(len(srcs))}
+    hashes = {r * len(srcs) + i: rows[r][i, 1:].tobytes() for r in range(world) for i in range(len(srcs))}
+    gpu_comp = [int(x) for r in range(world) for x in rows[r][:, 0]]
+    if args.no_validate:
+        valid, bad, comp, cpu = None, None, gpu_comp, None
+    else:
+        valid, bad, comp, cpu = check_against_reference(g, srcs_all, own, hashes, timed=len(srcs))
+        valid = valid and comp == gpu_comp
+    edges_per_rank_step = sum(comp[:len(srcs)])
+    edges_all = sum(comp)
     # reference summary: harmonic mean over sources of per-source GTEPS (src/bench/main.cpp:366-370)
     hmean = len(srcs) / sum((lm * 1e-3) / (c / 1e9) for lm, c in zip(launch_ms[: len(srcs)], comp) if c)
 
@@ -754,52 +949,102 @@ def main():
     bytes_per_trav = 4 * (g.n + 1) + 4 * g.m + 4 * g.n
     mean_launch = statistics.mean(launch_ms)
     achieved = bytes_per_trav / (mean_launch * 1e-3) / 1e9
-    traffic = measured_traffic("persistentBfsKernel", "rmat22_bfs64") if args.scale == SCALE else None
+    kernel = f"persistentBfsKernel<{opts.block or 512}>"
+    traffic = (measured_traffic(kernel, WORKLOAD, opts.grid_blocks) if args.scale == SCALE else None)
 
-    value = world * edges_per_step * args.steps / (total_ms * 1e-3) / 1e9
-    e2e_value = world * edges_per_step * args.steps / (e2e_total * 1e-3) / 1e9
-    e2e_distinct = world * edges_per_step * args.steps / (e2e_distinct_total * 1e-3) / 1e9
-    if rank != 0:
-        return
-    cpu = None
-    if not args.no_cpu_baseline and world == 1:
-        try:
-            cpu = cpu_baseline(g, srcs)
-        except Exception as e:  # reported, never fatal
-            cpu = {"value": None, "error": str(e)[:200]}
+    value = edges_all * args.steps / (total_ms * 1e-3) / 1e9
+    e2e_value = edges_all * args.steps / (e2e_total * 1e-3) / 1e9
+    e2e_distinct = edges_all * args.steps / (e2e_distinct_total * 1e-3) / 1e9
+    wire = int(depth_wire_bytes(g.n, max_levels) * g.n * len(srcs))
+    config = headline_config(g.n, g.m, world, len(srcs))
+    if args.scale != SCALE:
+        config["workload"] = f"rmat{args.scale}_bfs{len(srcs)}"
     line = {
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": WORKLOAD if args.scale == SCALE else f"rmat{args.scale}_bfs{len(srcs)}", "n": g.n, "m": g.m, "sources": len(srcs), "selector": selector,
-                   "adjacency": args.adjacency,
+        "config": config,
+        "method": {"selector": selector, "adjacency": args.adjacency,
                    "tuned": {"block": opts.block, "grid_blocks": opts.grid_blocks, "hub_min": opts.hub_min},
-                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (CSR 293 MB)",
-                   "edges_per_step": edges_per_step},
+                   "call": "gb_bfs_run_many, one persistent launch per source, back to back"},
+        "work": {"edges_per_step": edges_all, "edges_per_step_rank0": edges_per_rank_step,
+                 "teps_denominators": "component edges of the reference's cpu_do depths"},
         "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),
-                "d2h_bytes_per_step": int(depth_wire_bytes(g.n, max_levels) * g.n * len(srcs)),
-                "result_bytes_per_step": 4 * g.n * len(srcs)},
+                "d2h_bytes_per_step": wire, "result_bytes_per_step": 4 * g.n * len(srcs),
+                "host_output": "one pinned uint32[n] array reused by every source (as the reference's loop)"},
+        "e2e_distinct_buffers": {"value": e2e_distinct, "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),
+                                 "d2h_bytes_per_step": wire, "result_bytes_per_step": 4 * g.n * len(srcs),
+                                 "host_output": "a separate uint32[n] array per source (1 GB per step)"},
         "gpu_launches": len(srcs) * args.steps,
         "gpu_launches_e2e": 2 * len(srcs) * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": f"persistentBfsKernel<{opts.block or 512}>", "bytes_per_launch": bytes_per_trav,
-                     "mean_launch_ms": mean_launch},
-        "cpu_baseline": cpu,
+                     "kernel": kernel, "bytes_per_launch": bytes_per_trav,
+                     "mean_launch_ms": mean_launch,
+                     "dram_achieved": (traffic / (mean_launch * 1e-3) / 1e9) if traffic else None},
+        "cpu_baseline": cpu if world == 1 else None,
         "clocks": clocks.summary(),
-        "validated": bool(valid),
-        "compare": {"plain_gpu_do_gteps": edges_per_step / (plain_ms * 1e-3) / 1e9,
-                    "persistent_rule_gteps": edges_per_step / (rule_ms * 1e-3) / 1e9,
+        "validated": valid,
+        "validated_sources": (len(srcs_all) if valid else 0) if valid is not None else None,
+        "validation": ("every source's depths (from the timed e2e call) equal the reference's cpu_do "
+                       "(oracle/_ref) bit for bit" + ("; other ranks' by 128-bit digest" if world > 1 else "")),
+        "compare": {"plain_gpu_do_gteps": edges_per_rank_step / (plain_ms * 1e-3) / 1e9,
+                    "persistent_rule_gteps": edges_per_rank_step / (rule_ms * 1e-3) / 1e9,
                     "persistent_rule_tuned": ({"block": rule_opts.block, "grid_blocks": rule_opts.grid_blocks,
                                                "hub_min": rule_opts.hub_min} if rule_opts is not None else None),
-                    "persistent_learned_gteps": edges_per_step / (learned_ms * 1e-3) / 1e9,
+                    "persistent_learned_gteps": edges_per_rank_step / (learned_ms * 1e-3) / 1e9,
                     "speedup_learned_vs_rule": rule_ms / learned_ms,
                     "judge_ms_16_sources": {k: round(v[0], 4) for k, v in cands.items()},
                     "speedup_vs_plain_gpu_do": plain_ms / (total_ms / args.steps),
-                    "e2e_distinct_buffers_gteps": e2e_distinct, "e2e_distinct_buffers_exact": bool(distinct_ok),
                     "hmean_gteps_per_source": hmean},
     }
+    if bad is not None:
+        line["validation_failure"] = bad
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain/rule comparison runs")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the other benchmark configurations (road, Chung-Lu, web) after the headline")
+    ap.add_argument("--no-validate", action="store_true",
+                    help="skip the reference check of every depth array (profiling runs only; "
+                         "the line then says validated: null)")
+    ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (smaller: profiling cases)")
+    ap.add_argument("--sources", type=int, default=NSRC, help="sources per GPU")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=[WORKLOAD, "chunglu_pr20", "road_bfs", "chunglu_bfs64", "web_pr_tol", "snap_convert"],
+                    help="rmat22_bfs64 (default, the headline); chunglu_pr20, road_bfs, chunglu_bfs64, web_pr_tol, "
+                         "snap_convert")
+    ap.add_argument("--n", type=int, default=3070000, help="chunglu_pr20: vertices")
+    ap.add_argument("--adjacency", default="hub-first", choices=["hub-first", "natural"],
+                    help="BFS device adjacency layout (hub-first: lists by descending neighbour degree; same depths)")
+    args = ap.parse_args()
+    world, rank, local = init_dist(args)
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+        return
+    args.warmup = max(3, args.warmup)
+    workloads = {"chunglu_pr20": pagerank_workload, "road_bfs": bfs_config_workload,
+                 "chunglu_bfs64": bfs_config_workload, "web_pr_tol": pagerank_tol_workload,
+                 "snap_convert": snap_convert_workload, WORKLOAD: headline_workload}
+    line = workloads[args.workload](args, world, rank, local)
+    if line is None:
+        return
+    ok = line.get("validated") is not False
+    if args.workload == WORKLOAD and world == 1 and not args.no_secondary:
+        line["secondary"] = secondary_workloads(args, local)
+        ok = ok and all(v.get("validated") is not False for v in line["secondary"].values())
     print(json.dumps(line), flush=True)
+    if not ok:
+        log("VALIDATION FAILED: " + json.dumps(line.get("validation_failure")))
+        sys.exit(1)
 
 
 if __name__ == "__main__":

@@ -187,14 +187,16 @@ orc_csr* orc_gen_grid2d(uint32_t rows, uint32_t cols) {
 }
 
 /* src/graph/generators.cpp:51-75: per edge, `scale` quadrant draws with
- * a = .57, b = .19, c = .19 from one SplitMix64 stream. */
-orc_csr* orc_gen_rmat_edges(uint32_t scale, uint64_t m, int directed, uint64_t seed) {
+ * a = .57, b = .19, c = .19 from one SplitMix64 stream.  The raw endpoint
+ * pairs, before fromEdgeList (the reference's gen::rmat takes only an integer
+ * edge factor; this takes any edge count on the same stream). */
+void orc_rmat_draw(uint32_t scale, uint64_t m, uint64_t seed, uint32_t* eu, uint32_t* ev) {
     const double a = 0.57, b = 0.19, c = 0.19;
-    const uint64_t n = 1ull << scale;
-    uint64_t s = seed;
-    uint32_t* eu = (uint32_t*)xmalloc(m * sizeof(uint32_t));
-    uint32_t* ev = (uint32_t*)xmalloc(m * sizeof(uint32_t));
+    /* edge i takes draws i*scale+1 .. i*scale+scale of the stream, whose state
+     * before them is seed + i*scale*golden: edges are independent */
+#pragma omp parallel for schedule(static)
     for (uint64_t i = 0; i < m; ++i) {
+        uint64_t s = seed + i * (uint64_t)scale * 0x9E3779B97F4A7C15ull;
         uint32_t u = 0, v = 0;
         for (uint32_t bit = 0; bit < scale; ++bit) {
             double r = orc_rng_uniform(&s);
@@ -214,6 +216,13 @@ orc_csr* orc_gen_rmat_edges(uint32_t scale, uint64_t m, int directed, uint64_t s
         eu[i] = u;
         ev[i] = v;
     }
+}
+
+orc_csr* orc_gen_rmat_edges(uint32_t scale, uint64_t m, int directed, uint64_t seed) {
+    const uint64_t n = 1ull << scale;
+    uint32_t* eu = (uint32_t*)xmalloc((m ? m : 1) * sizeof(uint32_t));
+    uint32_t* ev = (uint32_t*)xmalloc((m ? m : 1) * sizeof(uint32_t));
+    orc_rmat_draw(scale, m, seed, eu, ev);
     orc_csr* g = orc_from_edge_list(n, eu, ev, m, directed);
     free(eu);
     free(ev);

@@ -63,6 +63,8 @@ orc_csr* orc_gen_grid2d(uint32_t rows, uint32_t cols);
 orc_csr* orc_gen_rmat(uint32_t scale, uint32_t edgefactor, int directed, uint64_t seed);
 /* R-MAT with an explicit generated-edge count (same quadrant draw). */
 orc_csr* orc_gen_rmat_edges(uint32_t scale, uint64_t edges, int directed, uint64_t seed);
+/* The raw R-MAT endpoint pairs of orc_gen_rmat_edges, before fromEdgeList. */
+void orc_rmat_draw(uint32_t scale, uint64_t edges, uint64_t seed, uint32_t* eu, uint32_t* ev);
 
 /* Transforms (src/graph/transform.cpp:9-76) and the random ordering
  * (src/graph/reorder.cpp:20-25). */

@@ -96,6 +96,7 @@ def lib():
             f.restype = P
         L.orc_csr_free.argtypes = [P]
         L.orc_random_perm.argtypes = [C.c_uint64, C.c_uint64, _u32p]
+        L.orc_rmat_draw.argtypes = [C.c_uint32, C.c_uint64, C.c_uint64, _u32p, _u32p]
         L.orc_validate.argtypes = [P]
         L.orc_validate.restype = C.c_int
         L.orc_bfs_serial.argtypes = [P, C.c_uint32, _u32p]
@@ -195,6 +196,15 @@ def symmetrize(g: HostGraph) -> HostGraph:
 
 def permute(g: HostGraph, perm: np.ndarray) -> HostGraph:
     return _take(lib().orc_permute(_View(g).ptr, np.ascontiguousarray(perm, np.uint32)))
+
+
+def rmat_draw(scale: int, edges: int, seed: int) -> tuple[np.ndarray, np.ndarray]:
+    """The raw R-MAT endpoint pairs (src/graph/generators.cpp:51-75 quadrant
+    draws, any edge count), before fromEdgeList."""
+    eu = np.zeros(max(edges, 1), dtype=np.uint32)
+    ev = np.zeros(max(edges, 1), dtype=np.uint32)
+    lib().orc_rmat_draw(scale, edges, seed, eu, ev)
+    return eu[:edges], ev[:edges]
 
 
 def random_perm(n: int, seed: int) -> np.ndarray:
@@ -329,7 +339,10 @@ REF_PATH = os.path.join(HERE, "_ref", "libgref.so")
 
 
 def ref_available() -> bool:
-    if not os.path.exists(REF_PATH) and os.path.isdir("/root/reference/src/cpu"):
+    """True when the reference build exists; otherwise tries `make ref` once
+    (the Makefile knows where the reference sources are and skips when they
+    are absent)."""
+    if not os.path.exists(REF_PATH):
         subprocess.run(["make", "-C", HERE, "ref"], check=False, capture_output=True)
     return os.path.exists(REF_PATH)
 
@@ -450,6 +463,26 @@ class RefGraph:
         it = ref().gref_pagerank(self.h, np.ascontiguousarray(outdeg, np.uint32), r, iters, tol,
                                  threads, C.byref(last))
         return r[:n], it, last.value
+
+
+def ref_rmat_graph(scale: int, edges: int, seed: int, perm_seed: int) -> RefGraph:
+    """An undirected R-MAT graph built by the reference's own code: the restated
+    quadrant draw (rmat_draw), then graph::fromEdgeList, reorder "random"
+    (perm_seed) and graph::permute -- how the benchmark graph of 2^22 vertices
+    and 8.5 * 2^22 drawn edges is defined."""
+    eu, ev = rmat_draw(scale, edges, seed)
+    r = RefGraph(ref().gref_from_edges(1 << scale, eu, ev, eu.size, 0))
+    del eu, ev
+    return r.permute(r.ordering("random", perm_seed))
+
+
+def ref_check_ranks(ref_ranks: np.ndarray, got: np.ndarray) -> PrCheck:
+    """The reference's own cpu::checkRanks (src/cpu/pagerank_cpu.hpp:37-60)."""
+    a, b, c = C.c_double(), C.c_double(), C.c_double()
+    ref().gref_check_ranks_f32(np.ascontiguousarray(ref_ranks, np.float64),
+                               np.ascontiguousarray(got, np.float32), ref_ranks.size,
+                               C.byref(a), C.byref(b), C.byref(c))
+    return PrCheck(a.value, b.value, c.value)
 
 
 def ref_suite(name: str) -> RefGraph:

@@ -1,9 +1,10 @@
 """gb_prim_scan_device_noalloc, the exclusive scan that allocates no device
-memory, checked through the C ABI against gb_prim_scan (the allocating entry
-point) on the same inputs.  Integer work, so the tolerance is exact equality.
-Several calls run back to back on one stream, so each must clear the fixed
-scratch the previous one left behind.  The file is named to be collected
-last; it also passes alone in a fresh process."""
+memory, checked through the C ABI against numpy's 64-bit cumulative sum
+(reduced mod 2^32, shifted to exclusive) and against gb_prim_scan (the
+allocating entry point) on the same inputs.  Integer work, so the tolerance is
+exact equality.  Several calls run back to back on one stream, so each must
+clear the fixed scratch the previous one left behind.  The file is named to be
+collected last; it also passes alone in a fresh process."""
 import numpy as np
 import pytest
 
@@ -25,6 +26,30 @@ def _scan_noalloc(gb, torch, x: np.ndarray, in_place: bool = False):
     return out, int(d_tot.cpu().numpy().view(np.uint32)[0]), int(d_flag.cpu()[0])
 
 
+def _numpy_scan(x: np.ndarray):
+    """Exclusive scan mod 2^32 and the total, independently of the library."""
+    c = np.cumsum(x, dtype=np.uint64)
+    want = np.empty(x.size, np.uint32)
+    if x.size:
+        want[0] = 0
+        want[1:] = (c[:-1] & 0xFFFFFFFF).astype(np.uint32)
+    return want, int(c[-1] & 0xFFFFFFFF) if x.size else 0
+
+
+def test_noalloc_scan_matches_numpy_at_the_limit(gb):
+    """n = 8,388,608 (4096 full tiles), full 32-bit values so the sums wrap,
+    out of place and in place."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(77)
+    x = rng.integers(0, 1 << 32, size=LIMIT, dtype=np.uint64).astype(np.uint32)
+    want, want_total = _numpy_scan(x)
+    for in_place in (False, True):
+        got, total, flag = _scan_noalloc(gb, torch, x, in_place)
+        assert flag == 0
+        np.testing.assert_array_equal(got, want)
+        assert total == want_total
+
+
 def test_noalloc_scan_matches_allocating_scan(gb):
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(2024)
@@ -38,6 +63,9 @@ def test_noalloc_scan_matches_allocating_scan(gb):
         assert flag == 0, n
         np.testing.assert_array_equal(got, want)
         assert total == want_total, n
+        np_want, np_total = _numpy_scan(x)
+        np.testing.assert_array_equal(got, np_want)
+        assert total == np_total, n
 
 
 def test_noalloc_scan_two_calls_in_a_row(gb):
@@ -48,6 +76,9 @@ def test_noalloc_scan_two_calls_in_a_row(gb):
     n = 5_000_000
     x = rng.integers(0, 1000, size=n, dtype=np.uint64).astype(np.uint32)
     want, want_total = gb.prim_scan(x)
+    np_want, np_total = _numpy_scan(x)
+    np.testing.assert_array_equal(want, np_want)
+    assert want_total == np_total
     d_in = torch.from_numpy(x.view(np.int32)).to("cuda")
     outs = [torch.empty_like(d_in), torch.empty_like(d_in)]
     tots = torch.zeros(2, dtype=torch.int32, device="cuda")
@@ -77,3 +108,25 @@ def test_noalloc_scan_limits(gb):
     gb.prim_scan_device_noalloc(buf.data_ptr(), 0, buf.data_ptr(), tot.data_ptr())
     torch.cuda.synchronize()
     assert int(tot.cpu()[0]) == 0
+
+
+def test_noalloc_scan_leaves_device_memory_unchanged(gb):
+    """After a first call (which looks up the scratch address), many more
+    calls leave the device's free memory exactly as it was: nothing is
+    allocated and kept per call."""
+    torch = pytest.importorskip("torch")
+    n = 1_000_003
+    d_in = torch.ones(n, dtype=torch.int32, device="cuda")
+    d_out = torch.empty_like(d_in)
+    d_tot = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream()
+    gb.prim_scan_device_noalloc(d_in.data_ptr(), n, d_out.data_ptr(), d_tot.data_ptr(), 0, s.cuda_stream)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(50):
+        gb.prim_scan_device_noalloc(d_in.data_ptr(), n, d_out.data_ptr(), d_tot.data_ptr(), 0, s.cuda_stream)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert int(d_tot.cpu()[0]) == n
+    assert int(d_out[-1].cpu()) == n - 1
