@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -170,8 +171,30 @@ void cpuBfsSerial(const Graph& g, uint32_t src, uint32_t* dist) {
     }
 }
 
+// cpu_omp's loop schedule (--schedule, src/cpu/bfs_cpu.hpp:16-19): the same
+// three choices and CSV names as the reference.
+enum class Schedule { Static, Dynamic64, Guided };
+
+Schedule parseSchedule(const std::string& s) {
+    if (s == "static") return Schedule::Static;
+    if (s == "dynamic" || s == "dynamic,64" || s == "dynamic/64") return Schedule::Dynamic64;
+    if (s == "guided") return Schedule::Guided;
+    throw std::runtime_error("unknown schedule '" + s + "' (static | dynamic,64 | guided)");
+}
+
+const char* scheduleName(Schedule s) {
+    return s == Schedule::Static ? "static" : s == Schedule::Guided ? "guided" : "dynamic/64";
+}
+
+void setSchedule(Schedule s) {
+    if (s == Schedule::Static) omp_set_schedule(omp_sched_static, 0);
+    else if (s == Schedule::Guided) omp_set_schedule(omp_sched_guided, 0);
+    else omp_set_schedule(omp_sched_dynamic, 64);
+}
+
 // Level-synchronous top-down with CAS claims; per-thread buffers are
-// concatenated after the parallel loop.
+// concatenated after the parallel loop.  The loop takes the schedule set by
+// setSchedule (dynamic,64 unless cpu_omp's --schedule says otherwise).
 uint64_t cpuTopDown(const Graph& g, uint32_t* dist, const std::vector<uint32_t>& front, std::vector<uint32_t>& next,
                     uint32_t d, int nt, uint64_t* scout) {
     std::vector<std::vector<uint32_t>> parts(nt);
@@ -179,7 +202,7 @@ uint64_t cpuTopDown(const Graph& g, uint32_t* dist, const std::vector<uint32_t>&
 #pragma omp parallel num_threads(nt) reduction(+ : sc)
     {
         std::vector<uint32_t>& local = parts[omp_get_thread_num()];
-#pragma omp for schedule(dynamic, 64)
+#pragma omp for schedule(runtime)
         for (int64_t i = 0; i < (int64_t)front.size(); ++i) {
             uint32_t u = front[i];
             for (uint32_t k = g.c.row_ptr[u]; k < g.c.row_ptr[u + 1]; ++k) {
@@ -199,7 +222,9 @@ uint64_t cpuTopDown(const Graph& g, uint32_t* dist, const std::vector<uint32_t>&
     return next.size();
 }
 
-void cpuBfsOmp(const Graph& g, uint32_t src, uint32_t* dist, int nt, std::vector<gpu::BfsLevel>* tr) {
+void cpuBfsOmp(const Graph& g, uint32_t src, uint32_t* dist, int nt, Schedule schedule,
+               std::vector<gpu::BfsLevel>* tr) {
+    setSchedule(schedule);
     std::fill(dist, dist + g.n(), kUnreached);
     dist[src] = 0;
     std::vector<uint32_t> front{src}, next;
@@ -216,6 +241,7 @@ void cpuBfsOmp(const Graph& g, uint32_t src, uint32_t* dist, int nt, std::vector
 // Direction-optimizing BFS: the rule of src/cpu/bfs_cpu.cpp:227-283.
 void cpuBfsDO(const Graph& g, uint32_t src, uint32_t* dist, double alpha, double beta, int nt,
               std::vector<gpu::BfsLevel>* tr) {
+    setSchedule(Schedule::Dynamic64);
     const uint64_t n = g.n();
     std::fill(dist, dist + n, kUnreached);
     dist[src] = 0;
@@ -355,6 +381,31 @@ std::string timestamp() {
     return b;
 }
 
+// Short hash of the checkout the binary runs from, "+" when tracked files
+// are modified, "unknown" outside a git checkout (the CSV's git_commit field,
+// src/util/sysinfo.hpp:27-42).
+std::string gitCommit() {
+    auto run = [](const char* cmd) {
+        std::string out;
+        if (FILE* p = popen(cmd, "r")) {
+            char buf[128];
+            while (std::fgets(buf, sizeof buf, p)) out += buf;
+            pclose(p);
+        }
+        while (!out.empty() && std::isspace((unsigned char)out.back())) out.pop_back();
+        return out;
+    };
+    std::string h = run("git rev-parse --short HEAD 2>/dev/null");
+    if (h.empty()) return "unknown";
+    if (!run("git status --porcelain --untracked-files=no 2>/dev/null").empty()) h += "+";
+    return h;
+}
+
+double loadAverage1() {
+    double l[3];
+    return getloadavg(l, 3) > 0 ? l[0] : -1;
+}
+
 std::string chipName() {
     char name[256] = "unknown";
     int sms = 0, ma = 0, mi = 0;
@@ -449,15 +500,23 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
     const int nt = threads > 0 ? threads : omp_get_max_threads();
     gpu::GpuBfsOptions o;
     o.tg = (uint32_t)args.getInt("tg", 256);
-    o.small_max = (uint32_t)args.getInt("small-max", 16);
-    o.large_min = (uint32_t)args.getInt("large-min", 256);
+    o.smallMax = (uint32_t)args.getInt("small-max", 16);
+    o.largeMin = (uint32_t)args.getInt("large-min", 256);
     o.ept = (uint32_t)args.getInt("ept", 2);
     o.alpha = args.getDouble("alpha", 15.0);
     o.beta = args.getDouble("beta", 18.0);
     o.block = (uint32_t)args.getInt("block", 512);
-    o.hub_min = (uint32_t)args.getInt("hub-min", 4096);
-    o.grid_blocks = (uint32_t)args.getInt("grid-blocks", 0);
-    o.sel_margin = (float)args.getDouble("sel-margin", o.sel_margin);
+    o.hubMin = (uint32_t)args.getInt("hub-min", 4096);
+    o.gridBlocks = (uint32_t)args.getInt("grid-blocks", 0);
+    o.selMargin = (float)args.getDouble("sel-margin", o.selMargin);
+    // --T: the reference's hybrid threshold (levels below it ran on the CPU).
+    // hybrid runs every level in the persistent kernel here, so the value is
+    // accepted, recorded in params and does not change what runs.
+    const std::string tArg = args.get("T", "100000");
+    o.hybridT = tArg == "inf" ? UINT64_MAX : (uint64_t)std::stoull(tArg);
+    o.cpuThreads = (variant == "hybrid" && !args.has("threads")) ? 4 : threads;
+    // --schedule: cpu_omp's OpenMP loop schedule (src/cpu/bfs_cpu.cpp:9-14)
+    const Schedule schedule = parseSchedule(args.get("schedule", "dynamic,64"));
     const std::string sel = args.get("selector", "rule");
     if (sel != "rule" && sel != "learned") throw std::runtime_error("--selector must be rule or learned");
     o.selector = sel == "learned" ? GB_SELECT_LEARNED : GB_SELECT_RULE;
@@ -512,7 +571,8 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
     using Fn = std::function<void(uint32_t, uint32_t*, std::vector<gpu::BfsLevel>*)>;
     Fn fn;
     if (variant == "cpu_serial") fn = [&](uint32_t s, uint32_t* d, std::vector<gpu::BfsLevel>*) { cpuBfsSerial(g, s, d); };
-    else if (variant == "cpu_omp") fn = [&](uint32_t s, uint32_t* d, std::vector<gpu::BfsLevel>* t) { cpuBfsOmp(g, s, d, nt, t); };
+    else if (variant == "cpu_omp")
+        fn = [&](uint32_t s, uint32_t* d, std::vector<gpu::BfsLevel>* t) { cpuBfsOmp(g, s, d, nt, schedule, t); };
     else if (variant == "cpu_do")
         fn = [&](uint32_t s, uint32_t* d, std::vector<gpu::BfsLevel>* t) { cpuBfsDO(g, s, d, o.alpha, o.beta, nt, t); };
     else if (variant == "gpu_vertex") fn = [&](uint32_t s, uint32_t* d, std::vector<gpu::BfsLevel>* t) { gbfs->runVertex(s, d, o, t); };
@@ -524,9 +584,10 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
 
     std::string params;
     if (variant == "cpu_omp" || variant == "cpu_do") params = "threads=" + std::to_string(nt);
+    if (variant == "cpu_omp") params += std::string(" schedule=") + scheduleName(schedule);
     if (gpuVariant) params = "tg=" + std::to_string(o.tg);
     if (variant == "gpu_binned")
-        params += " small_max=" + std::to_string(o.small_max) + " large_min=" + std::to_string(o.large_min);
+        params += " small_max=" + std::to_string(o.smallMax) + " large_min=" + std::to_string(o.largeMin);
     if (variant == "gpu_edge" || variant == "gpu_do") params += " ept=" + std::to_string(o.ept);
     if (variant == "gpu_do" || variant == "cpu_do" || variant == "gpu_do_persistent" || variant == "hybrid") {
         char b[96];
@@ -534,7 +595,9 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
         params += b;
     }
     if (variant == "gpu_do_persistent" || variant == "hybrid")
-        params += " selector=" + sel + " block=" + std::to_string(o.block) + " hub_min=" + std::to_string(o.hub_min);
+        params += " selector=" + sel + " block=" + std::to_string(o.block) + " hub_min=" + std::to_string(o.hubMin);
+    if (variant == "hybrid")
+        params += " T=" + tArg + " threads=" + std::to_string(o.cpuThreads > 0 ? o.cpuThreads : omp_get_max_threads());
     if (batch > 0) params += " batch=" + std::to_string(batch);
 
     std::printf("%s: n %llu, symmetrized m %llu (%llu undirected edges), prep %.0f ms\n", dataset.c_str(),
@@ -567,19 +630,15 @@ int runBfs(const Args& args, const Graph& stored, const std::string& dataset) {
             csv << "timestamp,git_commit,chip,dataset,n,m,ordering,algo,variant,params,source,trial,"
                    "time_ms_e2e,time_ms_gpu,gteps,iters,validated,load1\n";
     }
-    const std::string ts = timestamp(), chip = chipName();
-    double load1 = -1;
-    {
-        double l[3];
-        if (getloadavg(l, 3) > 0) load1 = l[0];
-    }
+    const std::string ts = timestamp(), chip = chipName(), commit = gitCommit();
+    const double load1 = loadAverage1();
     auto row = [&](uint32_t s, int t, double ms, double gpuMs, double gteps) {
         if (!csv.is_open()) return;
         char gpuField[32] = "";
         if (gpuMs >= 0) std::snprintf(gpuField, sizeof gpuField, "%.4f", gpuMs);
         char b[1024];
         std::snprintf(b, sizeof b, "%s,%s,%s,%s,%llu,%llu,%s,bfs,%s,%s,%u,%d,%.4f,%s,%.6f,,%d,%.2f\n", ts.c_str(),
-                      "unknown", chip.c_str(), dataset.c_str(), (unsigned long long)g.n(), (unsigned long long)g.m(),
+                      commit.c_str(), chip.c_str(), dataset.c_str(), (unsigned long long)g.n(), (unsigned long long)g.m(),
                       ordering.c_str(), variant.c_str(), params.c_str(), s, t, ms, gpuField, gteps, validate ? 1 : 0,
                       load1);
         csv << b;
@@ -720,12 +779,15 @@ int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
     o.iters = iters;
     o.tol = tol;
     o.tg = (uint32_t)args.getInt("tg", 256);
-    o.small_max = (uint32_t)args.getInt("small-max", 16);
-    o.large_min = (uint32_t)args.getInt("large-min", 256);
-    o.inplace = args.has("inplace") ? 1 : 0;
-    o.tol_rel = args.getDouble("tol-rel", 0);
+    o.smallMax = (uint32_t)args.getInt("small-max", 16);
+    o.largeMin = (uint32_t)args.getInt("large-min", 256);
+    o.inPlace = args.has("inplace");
+    o.tolRel = args.getDouble("tol-rel", 0);
     const bool validate = args.has("validate");
-    const bool gsCheck = variant == "gpu_pull_gs" || o.inplace;
+    const bool gsCheck = variant == "gpu_pull_gs" || o.inPlace;
+    // --ref-tol: the Jacobi reference's tolerance when it should differ from
+    // --tol (Gauss-Seidel at a tighter tol judged against Jacobi at 1e-6)
+    const double refTol = args.getDouble("ref-tol", tol);
 
     auto prep0 = std::chrono::steady_clock::now();
     // --ordering: perm from the symmetric graph, applied to the stored graph
@@ -759,6 +821,8 @@ int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
         for (uint64_t v = 0; v < stored.n(); ++v) odO[v] = stored.degree(v);
         double ld = 0;
         refIters = cpuPagerank(RI, odO, ref, iters, tol, nt, &ld);
+        if (gsCheck && refTol != tol)
+            refIters = cpuPagerank(RI, odO, ref, refTol > 0 ? 1000 : iters, refTol, nt, &ld);
         if (gsCheck) {
             cpuPagerank(RI, odO, refConv, 1000, 1e-10, nt, &ld);
             jacobiErr = checkRanks(refConv, ref.data());
@@ -770,7 +834,7 @@ int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
         gpr = std::make_unique<gpu::GpuPageRank>(G.n(), needOut ? G.c.row_ptr : nullptr,
                                                  needOut ? G.c.col_idx : nullptr, G.m(), in.c.row_ptr,
                                                  in.c.col_idx, in.m(), od);
-        if (variant == "gpu_pull_adaptive") gpr->prepareAdaptive(o.small_max, o.large_min);
+        if (variant == "gpu_pull_adaptive") gpr->prepareAdaptive(o.smallMax, o.largeMin);
         if (variant == "gpu_pull_gs") gpr->prepareGS((uint32_t)args.getInt("gs-pairs", 2));
     }
     const double prepMs = msSince(prep0);
@@ -780,7 +844,8 @@ int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
     std::vector<double> rcpu;
     const gpu::PrVariant pv = gpuVariant ? gpu::parsePrVariant(variant) : gpu::PrVariant::PullVector;
     int lastIters = 0;
-    double lastDelta = -1;
+    double lastDelta = -1, lastMaxRel = -1;
+    bool floorStop = false;
     auto runOnce = [&]() -> double {
         if (!gpuVariant) {
             lastIters = cpuPagerank(in, od, rcpu, iters, tol, variant == "cpu_serial" ? 1 : nt, &lastDelta);
@@ -788,8 +853,10 @@ int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
         }
         gpu::GpuPrResult r = gpr->run(pv, o);
         lastIters = r.iters;
-        lastDelta = r.last_delta;
-        return r.gpu_ms;
+        lastDelta = r.lastDelta;
+        lastMaxRel = r.lastMaxRel;
+        floorStop = r.floorStop;
+        return r.gpuMs;
     };
     auto ranksD = [&]() {  // original ids: rank of v = result[perm[v]]
         std::vector<double> out(stored.n()), r64;
@@ -804,6 +871,36 @@ int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
     };
     const int warmup = (int)args.getInt("warmup", 2), trials = (int)args.getInt("trials", 5);
     for (int w = 0; w < warmup; ++w) runOnce();
+
+    // CSV rows: one per trial, same schema as BFS (src/bench/main.cpp:571-620);
+    // source empty, gteps = m * iterations / time, iters = iterations run.
+    char tolStr[32];  // %g: tolerances below 1e-6 must not print as 0.000000
+    std::snprintf(tolStr, sizeof tolStr, "%g", tol);
+    std::string params = tol > 0 ? std::string("tol=") + tolStr + " cap=" + std::to_string(iters)
+                                 : "iters=" + std::to_string(iters);
+    if (variant == "cpu_omp") params += " threads=" + std::to_string(nt);
+    if (gpuVariant) params += " tg=" + std::to_string(o.tg);
+    if (o.tolRel > 0) {
+        char r[32];
+        std::snprintf(r, sizeof r, " tol_rel=%g", o.tolRel);
+        params += r;
+    }
+    if (o.inPlace) params += " inplace";
+    if (variant == "gpu_pull_adaptive")
+        params += " small_max=" + std::to_string(o.smallMax) + " large_min=" + std::to_string(o.largeMin);
+    const std::string csvPath = args.get("csv", "");
+    const std::string ordering = args.get("ordering", "original");
+    std::ofstream csv;
+    if (!csvPath.empty()) {
+        bool fresh = !fileExists(csvPath);
+        csv.open(csvPath, std::ios::app);
+        if (fresh)
+            csv << "timestamp,git_commit,chip,dataset,n,m,ordering,algo,variant,params,source,trial,"
+                   "time_ms_e2e,time_ms_gpu,gteps,iters,validated,load1\n";
+    }
+    const std::string ts = timestamp(), chip = chipName(), commit = gitCommit();
+    const double load1 = loadAverage1();
+
     std::vector<double> times, gpuTimes;
     PrCheck worst;
     for (int t = 0; t < trials; ++t) {
@@ -823,13 +920,26 @@ int runPr(const Args& args, const Graph& stored, const std::string& dataset) {
         }
         times.push_back(ms);
         if (gms >= 0) gpuTimes.push_back(gms);
+        if (csv.is_open()) {
+            char gpuField[32] = "";
+            if (gms >= 0) std::snprintf(gpuField, sizeof gpuField, "%.4f", gms);
+            char row[1024];
+            std::snprintf(row, sizeof row, "%s,%s,%s,%s,%llu,%llu,%s,pr,%s,%s,,%d,%.4f,%s,%.6f,%d,%d,%.2f\n",
+                          ts.c_str(), commit.c_str(), chip.c_str(), dataset.c_str(), (unsigned long long)stored.n(),
+                          (unsigned long long)stored.m(), ordering.c_str(), variant.c_str(), params.c_str(), t, ms,
+                          gpuField, (double)stored.m() * lastIters / (ms * 1e6), lastIters, validate ? 1 : 0, load1);
+            csv << row;
+        }
     }
     if (!times.empty()) {
         const double med = median(times), perIt = med / std::max(1, lastIters);
         std::printf("time ms: median %.3f, min %.3f | %d iterations, %.4f ms/iteration", med,
                     *std::min_element(times.begin(), times.end()), lastIters, perIt);
         if (!gpuTimes.empty()) std::printf(" (GPU-only %.4f)", median(gpuTimes) / std::max(1, lastIters));
-        if (tol > 0) std::printf(" | final L1 change %.3g", lastDelta);
+        if (tol > 0)
+            std::printf(" | final L1 change %.3g%s", lastDelta,
+                        lastDelta < tol ? "" : floorStop ? " (stopped at float precision floor)" : " (NOT converged)");
+        if (tol > 0 && lastMaxRel >= 0) std::printf(", max rel change %.3g", lastMaxRel);
         const double bytes = 4.0 * (stored.n() + 1) + 8.0 * stored.m() + 4.0 * stored.n();
         std::printf(" | eff. %.1f GB/s", bytes / (perIt * 1e6));
         if (validate) std::printf(" | validated OK (ref %d iters; worst L1 %.2e)", refIters, worst.l1);

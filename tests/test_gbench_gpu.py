@@ -20,19 +20,14 @@ def _run(tmp_path, tag, args, host):
     out = tmp_path / f"{tag}_{'host' if host else 'gpu'}"
     out.mkdir()
     bfs = "bfs" in args
-    cmd = [GBENCH, *args, "--validate"]
-    if bfs:  # the PageRank path writes no CSV rows
-        cmd += ["--csv", str(out / "r.csv"), "--dump-dist", str(out / "d.bin")]
-    else:
-        cmd += ["--dump-ranks", str(out / "d.bin")]
+    cmd = [GBENCH, *args, "--validate", "--csv", str(out / "r.csv")]
+    cmd += ["--dump-dist" if bfs else "--dump-ranks", str(out / "d.bin")]
     if host:
         cmd.append("--host-prep")
     p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stdout + p.stderr
-    rows = []
-    if bfs:
-        with open(out / "r.csv") as f:
-            rows = list(csv.DictReader(f))
+    with open(out / "r.csv") as f:
+        rows = list(csv.DictReader(f))
     return rows, (out / "d.bin").read_bytes()
 
 
@@ -57,6 +52,12 @@ CASES = {
                                "--ordering", "rcm", "--iters", "20", "--trials", "1"],
     "rmat12_directed_degree_gs": ["--graph", "synth:rmat12_directed", "--algo", "pr", "--variant", "gpu_pull_gs",
                                   "--ordering", "degree", "--tol", "1e-6", "--trials", "1"],
+    # --ref-tol: Gauss-Seidel at a tighter tol judged against the Jacobi reference at 1e-6
+    "rmat12_directed_gs_ref_tol": ["--graph", "synth:rmat12_directed", "--algo", "pr", "--variant", "gpu_pull_gs",
+                                   "--tol", "1e-8", "--ref-tol", "1e-6", "--trials", "1"],
+    # --T: the reference's hybrid threshold, accepted; hybrid runs the persistent kernel
+    "rmat12_hybrid_T": ["--graph", "synth:rmat12", "--algo", "bfs", "--variant", "hybrid", "--T", "5000",
+                        "--sources", "4", "--trials", "1"],
 }
 
 
@@ -66,7 +67,8 @@ def test_gbench_gpu_prep_matches_host_prep(tmp_path, tag):
         pytest.fail("gbench is not built")
     rows_g, dump_g = _run(tmp_path, tag, CASES[tag], host=False)
     rows_h, dump_h = _run(tmp_path, tag, CASES[tag], host=True)
-    assert len(rows_g) == len(rows_h)
+    assert len(rows_g) == len(rows_h) > 0
+    assert all(r["validated"] == "1" for r in rows_g)
     assert [r["source"] for r in rows_g] == [r["source"] for r in rows_h]
     assert [(r["n"], r["m"]) for r in rows_g] == [(r["n"], r["m"]) for r in rows_h]
     if "bfs" in CASES[tag]:
@@ -76,6 +78,7 @@ def test_gbench_gpu_prep_matches_host_prep(tmp_path, tag):
         assert (d == 0).sum() == 1  # the dumped source
     else:
         # ranks: FP32 sweeps whose block sums may combine in either order
+        assert all(r["algo"] == "pr" and r["source"] == "" and int(r["iters"]) > 0 for r in rows_g)
         a, b = np.frombuffer(dump_g, np.float64), np.frombuffer(dump_h, np.float64)
         assert a.size == b.size > 0
         assert np.abs(a - b).sum() < 1e-6
