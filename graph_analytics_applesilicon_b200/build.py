@@ -52,8 +52,6 @@ def _compile(src: str, force: bool, verbose: bool, extra: list[str]) -> str:
     if not force and not _stale(obj, [src] + _headers()):
         return obj
     cmd = [nvcc(), "-c", src, "-o", obj] + NVCC_FLAGS + extra
-    if src.endswith(".cpp"):
-        cmd[3:3] = ["-x", "cu"] if False else []
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
