@@ -325,6 +325,13 @@ def secondary_workloads(args, local):
     return out
 
 
+def fixed_options(G, spec, selector):
+    """--fixed-opts BLOCK,GRID,HUB: the persistent / batched kernels' launch
+    shape and hub cut, given instead of tuned (profiling runs)."""
+    block, grid, hub = (int(x) for x in spec.split(","))
+    return G.BfsOptions(selector=selector, block=block, grid_blocks=grid, hub_min=hub)
+
+
 def headline_config(n, m, world, per_rank):
     """The workload description both arms print (identical keys and values)."""
     return {"workload": WORKLOAD, "graph": "rmat scale 22, 8.5*2^22 drawn edges (seed 22), ids permuted (seed 1)",
@@ -423,11 +430,16 @@ def bfs_config_workload(args, world, rank, local, g=None):
     if sel2 is not None:
         bfs.set_selector(sel2, 1)
     o1 = G.BfsOptions(selector="learned" if sel1 is not None else "rule")
-    o1 = bfs.autotune("gpu_do_persistent", srcs64[:2], o1)
+    o1 = fixed_options(G, args.fixed_opts, o1.selector) if args.fixed_opts else \
+        bfs.autotune("gpu_do_persistent", srcs64[:2], o1)
     # the batch runs with whichever selector (learned or the alpha/beta rule)
     # is faster on this graph after tuning block size, hub cut and grid size
     batch_cands = {}
     for sel in (("rule", "learned") if sel2 is not None else ("rule",)):
+        if args.fixed_opts:  # profiling runs: the launch shape given, no tuning launches
+            if sel == args.selector:
+                batch_cands[sel] = (0.0, fixed_options(G, args.fixed_opts, sel))
+            continue
         ob_ = bfs.autotune("batch", srcs64, G.BfsOptions(selector=sel))
         bfs.run_batch(srcs64, opts=ob_)
         bfs.run_batch(srcs64, opts=ob_)
@@ -849,6 +861,12 @@ def headline_workload(args, world, rank, local):
     # unless the tuned rule is faster on these sources (untimed)
     cands = {}
     for name in (("learned", "rule") if sel is not None else ("rule",)):
+        if args.fixed_opts:  # profiling runs: the launch shape given, no tuning launches
+            if name != args.selector:
+                continue
+            o = fixed_options(G, args.fixed_opts, name)
+            cands[name] = (0.0, o)
+            continue
         o = bfs.autotune("gpu_do_persistent", srcs[:4], G.BfsOptions(selector=name))
         for s_ in srcs[:16]:
             bfs.run("gpu_do_persistent", int(s_), opts=o)
@@ -857,7 +875,7 @@ def headline_workload(args, world, rank, local):
             bfs.run("gpu_do_persistent", int(s_), opts=o)
             t_ += bfs.lastGpuMs()
         cands[name] = (t_, o)
-    if world > 1:  # every rank must run the same selector and options
+    if world > 1 and not args.fixed_opts:  # every rank must run the same selector and options
         import torch.distributed as dist
         votes = torch.tensor([cands[k][0] for k in sorted(cands)], dtype=torch.float64, device="cuda")
         dist.all_reduce(votes, op=dist.ReduceOp.SUM)
@@ -934,7 +952,7 @@ def headline_workload(args, world, rank, local):
         if plain is not bfs:
             plain.close()
         # each selector in the same kernel, tuned the same way
-        rule_opts = cands["rule"][1]
+        rule_opts = cands["rule"][1] if "rule" in cands else opts
         device_step("gpu_do_persistent", rule_opts)
         rule_ms = device_step("gpu_do_persistent", rule_opts)[0]
         if "learned" in cands:
@@ -1029,6 +1047,11 @@ def main():
     ap.add_argument("--no-validate", action="store_true",
                     help="skip the reference check of every depth array (profiling runs only; "
                          "the line then says validated: null)")
+    ap.add_argument("--fixed-opts", default="",
+                    help="BLOCK,GRID,HUB: run the persistent / batched kernels with this launch shape and hub cut "
+                         "instead of autotuning (profiling runs)")
+    ap.add_argument("--selector", default="rule", choices=["rule", "learned"],
+                    help="with --fixed-opts: the per-level selector")
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (smaller: profiling cases)")
     ap.add_argument("--sources", type=int, default=NSRC, help="sources per GPU")
     ap.add_argument("--workload", default=WORKLOAD,

@@ -67,6 +67,8 @@ struct gb_bfs {
     gb::DevBuf<unsigned long long> phubOff[2];
     gb::DevBuf<uint32_t> pbm[3];         // frontier bitmaps
     gb::DevBuf<uint32_t> pvisited;       // visited bitmap
+    gb::DevBuf<uint32_t> pIso;           // degree-0 vertices, a bit each (visited from the start)
+    bool pIsoReady = false;
     gb::DevBuf<GbPCounters> pctr;        // [3]
     gb::DevBuf<unsigned> pctl;           // [0] barrier, [1] error, [2] levels, [3] flags
     gb::DevBuf<gb_level> ptrace;

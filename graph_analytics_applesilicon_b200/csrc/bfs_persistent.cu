@@ -45,6 +45,7 @@ struct PArgs {
     unsigned long long* ho[2];
     uint32_t* bm[3];
     uint32_t* visited;
+    const uint32_t* iso;  // bit per vertex of degree 0, or null
     GbPCounters* ctr;
     unsigned* ctl;  // [0] barrier word, [1] error flag, [2] levels run
     gb_level* trace;
@@ -239,8 +240,12 @@ __device__ __forceinline__ void tdGroups(const PArgs& a, uint32_t S, unsigned G,
     }
 }
 
-// One chunk of the hubs' concatenated edge space, split over the block; two
-// edges per thread per round so their loads overlap.
+// One chunk of the hubs' concatenated edge space, split over the block:
+// kHubEdges edges per thread in one round (kHubEdges NT edges per chunk), so
+// a thread's column reads, visited reads and claims are in flight together
+// and a large hub level takes few dependent rounds per block.
+constexpr int kHubEdges = 4;
+
 template <int NT>
 __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e1, uint32_t H, uint32_t qc,
                            uint32_t level, GbPCounters* cur, uint32_t* bmNext, Acc& acc, bool pre, bool enq) {
@@ -252,11 +257,11 @@ __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e
     }
     __syncthreads();
     const uint32_t lo = sm.range[0], hi = sm.range[1];
-    for (uint64_t base = e0; base < e1; base += 2 * NT) {
-        uint32_t u[2];
-        bool has[2];
+    for (uint64_t base = e0; base < e1; base += kHubEdges * NT) {
+        uint32_t u[kHubEdges];
+        bool has[kHubEdges];
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < kHubEdges; ++k) {
             const uint64_t e = base + k * NT + threadIdx.x;
             has[k] = e < e1;
             u[k] = 0;
@@ -265,8 +270,7 @@ __device__ void tdHubChunk(const PArgs& a, Smem<NT>& sm, uint64_t e0, uint64_t e
                 u[k] = a.col_idx[a.hs[qc][o] + (uint32_t)(e - ho[o])];
             }
         }
-#pragma unroll
-        discoverN<2>(a, has, u, level, cur, bmNext, qc ^ 1u, acc, pre, enq);
+        discoverN<kHubEdges>(a, has, u, level, cur, bmNext, qc ^ 1u, acc, pre, enq);
     }
     __syncthreads();
 }
@@ -438,7 +442,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
             uint32_t pad = 0;
             if (w == a.words - 1 && (a.n & 31)) pad = ~((1u << (a.n & 31)) - 1u);  // bits past n read as visited
             const uint32_t srcBit = w == (src >> 5) ? 1u << (src & 31) : 0u;
-            a.visited[w] = pad | srcBit;
+            // vertices of degree 0 start as visited: no edge reaches them (their
+            // depth stays infinity from the memset), and a bottom-up round then
+            // skips a bitmap word as soon as its other vertices are reached
+            a.visited[w] = pad | srcBit | (a.iso ? a.iso[w] : 0u);
             a.bm[0][w] = srcBit;
             a.bm[1][w] = 0;
         }
@@ -609,16 +616,20 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
                 parts = perPart < 1 ? 1u : (uint32_t)(perPart < cap ? perPart : cap);
             }
             const uint32_t nti = nt * parts;
-            const uint64_t HC = (uint64_t)NT * 2;
+            const uint64_t HC = (uint64_t)NT * kHubEdges;
             const bool pre = fedges >= 65536;
             const uint32_t nh = (uint32_t)((HE + HC - 1) / HC);
             uint32_t* bmNext = a.bm[(level + 1) % 3];
             // block b takes item b first; further items come from a ticket
-            // (none when the first items cover the level)
+            // (none when the first items cover the level), which thread 0
+            // requests while the block still works on the current item
             const bool oneRound = nti + nh <= gridDim.x;
-            for (bool first = true;; first = false) {
-                if (tid == 0)
-                    sm.item = first ? blockIdx.x : oneRound ? ~0u : gridDim.x + atomicAdd(&cur->work, 1u);
+            uint32_t nextItem = blockIdx.x;
+            for (;;) {
+                if (tid == 0) {
+                    sm.item = nextItem;
+                    nextItem = (oneRound || nextItem >= nti + nh) ? ~0u : gridDim.x + atomicAdd(&cur->work, 1u);
+                }
                 __syncthreads();
                 const uint32_t item = sm.item;
                 __syncthreads();
@@ -693,6 +704,25 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
     }
 }
 
+// Bit v of word v / 32: vertex v has no adjacency entries (row_ptr[v] ==
+// row_ptr[v + 1]); bits past n are 0.
+__global__ void isolatedBitmapKernel(const uint32_t* __restrict__ row_ptr, uint64_t n, uint32_t words,
+                                     uint32_t* out) {
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words;
+         w += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t bits = 0;
+        const uint64_t v0 = w * 32;
+        const uint32_t cnt = (uint32_t)(n - v0 < 32 ? n - v0 : 32);
+        uint32_t prev = row_ptr[v0];
+        for (uint32_t i = 0; i < cnt; ++i) {
+            const uint32_t next = row_ptr[v0 + i + 1];
+            if (next == prev) bits |= 1u << i;
+            prev = next;
+        }
+        out[w] = bits;
+    }
+}
+
 template <int NT>
 void launchPersistent(gb_bfs& h, PArgs& a) {
     void* args[] = {&a};
@@ -714,6 +744,7 @@ PArgs makeArgs(gb_bfs& h, const gb_bfs_options& o, uint32_t src) {
     }
     for (int i = 0; i < 3; ++i) a.bm[i] = h.pbm[i].get();
     a.visited = h.pvisited.get();
+    a.iso = h.pIso.get();
     a.ctr = h.pctr.get();
     a.ctl = h.pctl.get();
     a.trace = h.ptrace.get();
@@ -758,6 +789,13 @@ void gb_bfs::ensurePersistent(const gb_bfs_options& o) {
     const uint64_t words = (n + 31) / 32;
     for (auto& b : pbm) b.ensure(words);
     pvisited.ensure(words);
+    if (!pIsoReady) {  // degrees never change for a handle (hub-first only reorders lists)
+        pIso.ensure(words);
+        isolatedBitmapKernel<<<(uint32_t)std::min<uint64_t>((words + 255) / 256, 4096), 256, 0, stream.s>>>(
+            rowPtr.get(), n, (uint32_t)words, pIso.get());
+        GB_LAUNCH_CHECK();
+        pIsoReady = true;
+    }
     pctr.ensure(3);
     pctl.ensure(4);
     ptrace.ensure(kTraceCap);

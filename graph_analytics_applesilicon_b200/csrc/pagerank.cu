@@ -590,198 +590,122 @@ __global__ void prPushFinalizeKernel(PrArgs a) {
 }
 
 // ---------------------------------------------------------------- blocked pull
-// One CUDA block per SM: one producer warp and kBlkWarps consumer warps.
-// For each of the block's row blocks the producer walks the column parts
-// (starting at a part that depends on the row block, so the SMs do not all
-// stage the same contributions at once) through a ring of kBlkStages
-// shared-memory stages.  Each stage is filled by two TMA bulk copies
-// (cp.async.bulk, completion counted on the stage's "full" mbarrier): the
-// part's 32 KB of contributions and the row block's edge group for that
-// part.  Consumer warp w owns a fixed slice of the row block's rows; the
-// group header gives the range of its edges.  It takes 32 edges at a time,
-// adds equal-row neighbours with a shuffle scan and adds each run into the
-// row's shared-memory sum with a plain read-modify-write (no other warp
-// touches those rows), then arrives on the stage's "empty" mbarrier; the
-// producer refills a stage once all consumer warps have arrived.  Gathers
-// and edge reads come from shared memory, no block-wide barrier separates
-// parts, and each SM reads the contribution array once per iteration.  Row
-// sums are plain FP32 (fewer than kBlkHub terms); rows with more in-edges are
-// summed afterwards by one block each with Kahan-compensated per-thread sums
-// combined as float-float.  Every mbarrier wait is bounded: on a timeout the
-// block records the error in the control block and leaves without writing.
+// Rows in row blocks whose sums live in shared memory, columns in parts of
+// kBlkPart vertices whose contributions are staged in shared memory, so no
+// gather reaches L2: an edge costs one 4-byte streaming read from DRAM, one
+// shared-memory gather and one shared-memory float atomic add.  One CUDA
+// block of kBlkThreads per row block (one per SM at the graph sizes this form
+// is for), looping over the column parts starting at a part that depends on
+// the row block (the SMs then stage different contributions at once).  Part
+// j + 1's contributions are copied into the other half of a two-part ring by
+// cp.async while part j's edges are summed, and every thread holds the first
+// kBlkEdgeRegs 16-byte words of its share of part j + 1's edges in registers
+// by then, so one block barrier per part separates the parts and the copies
+// and loads of the next part overlap this part's work.  Every thread takes
+// an equal share of each tile's edges (no row ownership, so no warp waits for
+// another's heavier rows).  Rows with kBlkHub or more in-edges are summed
+// afterwards by one block each with Kahan-compensated per-thread sums
+// combined as float-float; the other rows' sums are plain FP32 (fewer than
+// kBlkHub terms).
 struct BlkArgs {
-    const uint32_t* edges;  // groups: kBlkHdr-word header, then packed edges
-    const uint32_t* off;    // word offset of group (k, p) at k * nParts + p
+    const uint4* edges;     // tiles of packed (row in block << 16 | column in part) words, 0xFFFFFFFF padding
+    const uint32_t* off;    // 16-byte-word offset of tile (k, p) at k * nParts + p, then the end
     const uint32_t* hubs;
     uint32_t nRowBlocks, rowsPer, nParts, nHubs;
-    unsigned long long spinLimit;
 };
 
-__device__ __forceinline__ uint32_t smemAddr(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
+__device__ __forceinline__ void cpAsync16(float* dst, const float* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ uint4 ldStream16(const uint4* p) {
+    uint4 v;
+    asm("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+        : "l"(p));
+    return v;
 }
 
-__device__ __forceinline__ void bulkLoad(void* dst, const void* src, uint32_t bytes, unsigned long long* mbar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smemAddr(dst)),
-        "l"(src), "r"(bytes), "r"(smemAddr(mbar))
-        : "memory");
-}
-
-// Wait for the given phase parity of mbar; gives up after `limit` polls.
-__device__ __forceinline__ bool blkWait(unsigned long long* mbar, uint32_t parity, unsigned long long limit) {
-    const uint32_t addr = smemAddr(mbar);
-    for (unsigned long long i = 0; i < limit; ++i) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(addr), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
+// The four edges of one 16-byte word into the row sums.
+__device__ __forceinline__ void blkAdd(float* sums, const float* part, uint4 w) {
+    if (w.x != 0xFFFFFFFFu) atomicAdd(&sums[w.x >> 16], part[w.x & 0xFFFFu]);
+    if (w.y != 0xFFFFFFFFu) atomicAdd(&sums[w.y >> 16], part[w.y & 0xFFFFu]);
+    if (w.z != 0xFFFFFFFFu) atomicAdd(&sums[w.z >> 16], part[w.z & 0xFFFFu]);
+    if (w.w != 0xFFFFFFFFu) atomicAdd(&sums[w.w >> 16], part[w.w & 0xFFFFu]);
 }
 
 __global__ void __launch_bounds__(kBlkThreads, 1) prBlockedKernel(PrArgs a, BlkArgs b) {
-    static_assert(kBlkThreads == 32 * (kBlkWarps + 1), "one producer warp and kBlkWarps consumer warps");
-    // stage s: contributions at s * kBlkPart, group words at kBlkStages * kBlkPart + s * kBlkEdgeBuf;
-    // row sums after the stages
-    extern __shared__ __align__(128) float blkSmem[];
-    __shared__ __align__(8) unsigned long long fullBar[kBlkStages], emptyBar[kBlkStages];
-    __shared__ int sErr;
+    // [0, 2 kBlkPart): the contribution ring; then the row block's sums
+    extern __shared__ __align__(16) float blkSmem[];
     const GbPrControl* c = a.ctl;
     if (ldvi(&c->stopped)) return;
     const int cur = c->cur;
     const bool withDelta = c->withDelta;
     const float dang = c->dangHi + c->dangLo;
     const float* contrib = a.contrib[cur];
-    uint32_t* gbase = reinterpret_cast<uint32_t*>(blkSmem + kBlkStages * kBlkPart);
-    float* sums = blkSmem + kBlkStages * (kBlkPart + kBlkEdgeBuf);
-    const unsigned tid = threadIdx.x, lane = laneId(), warp = tid >> 5;
+    float* sums = blkSmem + 2 * kBlkPart;
+    const unsigned tid = threadIdx.x;
     IterAcc acc;
-    if (tid == 0) {
-        for (uint32_t s = 0; s < kBlkStages; ++s) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(&fullBar[s])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(&emptyBar[s])), "r"(kBlkWarps)
-                         : "memory");
-        }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        sErr = 0;
-    }
-    __syncthreads();
-    auto rotation = [&](uint32_t k) { return (uint32_t)((uint64_t)k * b.nParts / b.nRowBlocks); };
-    if (warp == 0) {
-        // producer: lane 0 stages every (row block, part) of this block in order
-        if (lane == 0) {
-            uint32_t t = 0;  // fills issued so far (stage t % kBlkStages)
-            bool ok = true;
-            for (uint32_t k = blockIdx.x; k < b.nRowBlocks && ok; k += gridDim.x) {
-                const uint32_t rot = rotation(k);
-                auto partAt = [&](uint32_t j) { return j + rot < b.nParts ? j + rot : j + rot - b.nParts; };
-                // group bounds of the next fill, loaded one fill ahead
-                uint64_t gn = (uint64_t)k * b.nParts + partAt(0);
-                uint32_t nb0 = b.off[gn], nb1 = b.off[gn + 1];
-                for (uint32_t j = 0; j < b.nParts; ++j, ++t) {
-                    const uint32_t p = partAt(j);
-                    const uint32_t s = t % kBlkStages;
-                    const uint32_t g0 = nb0, words = min(nb1 - nb0, kBlkEdgeBuf);
-                    if (j + 1 < b.nParts) {
-                        gn = (uint64_t)k * b.nParts + partAt(j + 1);
-                        nb0 = b.off[gn];
-                        nb1 = b.off[gn + 1];
-                    }
-                    if (!blkWait(&emptyBar[s], ((t / kBlkStages) & 1u) ^ 1u, b.spinLimit)) {
-                        ok = false;
-                        break;
-                    }
-                    const uint32_t first = p * kBlkPart;
-                    const uint32_t cbytes = (min(kBlkPart, a.n - first) * 4u + 15u) & ~15u;
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                                     smemAddr(&fullBar[s])),
-                                 "r"(cbytes + words * 4u)
-                                 : "memory");
-                    bulkLoad(blkSmem + s * kBlkPart, contrib + first, cbytes, &fullBar[s]);
-                    bulkLoad(gbase + s * kBlkEdgeBuf, b.edges + g0, words * 4u, &fullBar[s]);
-                }
-            }
-            if (!ok) {
-                atomicOr(&a.ctl->error, 1);
-                sErr = 1;
-            }
-            // let every issued fill land before the block can leave
-            for (uint32_t s = 0; s < kBlkStages && t > s; ++s) {
-                const uint32_t last = t - 1 - ((t - 1 - s) % kBlkStages);  // last fill of stage s
-                blkWait(&fullBar[s], (last / kBlkStages) & 1u, b.spinLimit);
-            }
-        }
-        __syncwarp();
-    } else {
-        // consumer warp cw owns rows [ceil(cw R / W), ceil((cw + 1) R / W)) of each row block
-        const uint32_t cw = warp - 1;
-        uint32_t t = 0;
-        bool ok = true;
-        for (uint32_t k = blockIdx.x; k < b.nRowBlocks && ok; k += gridDim.x) {
-            const uint32_t r0 = k * b.rowsPer, rows = min(a.n, r0 + b.rowsPer) - r0;
-            const uint32_t lo = min(rows, (uint32_t)(((uint64_t)cw * b.rowsPer + kBlkWarps - 1) / kBlkWarps));
-            const uint32_t hi = min(rows, (uint32_t)(((uint64_t)(cw + 1) * b.rowsPer + kBlkWarps - 1) / kBlkWarps));
-            for (uint32_t i = lo + lane; i < hi; i += 32) sums[i] = 0.0f;
-            __syncwarp();
-            const uint32_t rot = rotation(k);
-            for (uint32_t j = 0; j < b.nParts; ++j, ++t) {
-                const uint32_t s = t % kBlkStages;
-                if (!blkWait(&fullBar[s], (t / kBlkStages) & 1u, b.spinLimit)) {
-                    ok = false;
-                    break;
-                }
-                const float* cbuf = blkSmem + s * kBlkPart;
-                const uint32_t* grp = gbase + s * kBlkEdgeBuf;
-                const uint32_t ws = grp[cw], wEnd = grp[cw + 1];  // header word kBlkWarps is the edge count
-                // edges past the staged words are read from global memory
-                const uint32_t p = j + rot < b.nParts ? j + rot : j + rot - b.nParts;
-                const uint32_t* gsrc = nullptr;
-                if (kBlkHdr + wEnd > kBlkEdgeBuf) gsrc = b.edges + b.off[(uint64_t)k * b.nParts + p];
-                for (uint32_t base = ws; base < wEnd; base += 32) {
-                    const uint32_t i = base + lane, w = kBlkHdr + i;
-                    const uint32_t q = i < wEnd ? (w < kBlkEdgeBuf ? grp[w] : ldStream(gsrc + w)) : 0xFFFFFFFFu;
-                    const bool real = q != 0xFFFFFFFFu;
-                    const uint32_t row = real ? (q >> 16) : 0x10000u + lane;  // padding: a run of its own
-                    float val = real ? cbuf[q & 0xFFFFu] : 0.0f;
-                    const uint32_t nextRow = __shfl_down_sync(kFull, row, 1);
-                    const bool runEnd = lane == 31 || nextRow != row;
-                    if (__all_sync(kFull, runEnd)) {  // usual case: every lane is its own run
-                        if (real) sums[row] += val;
-                    } else {
+    for (uint32_t k = blockIdx.x; k < b.nRowBlocks; k += gridDim.x) {
+        const uint32_t r0 = k * b.rowsPer, rows = min(a.n - r0, b.rowsPer);
+        for (uint32_t i = tid; i < rows; i += kBlkThreads) sums[i] = 0.0f;
+        const uint32_t rot = (uint32_t)((uint64_t)k * b.nParts / b.nRowBlocks);
+        auto partAt = [&](uint32_t j) { return j + rot < b.nParts ? j + rot : j + rot - b.nParts; };
+        // part p's contributions into ring half h: 16-byte copies (the
+        // contribution arrays carry 4 floats of slack past n)
+        auto stage = [&](uint32_t p, uint32_t h) {
+            const uint32_t first = p * kBlkPart, chunks = (min(kBlkPart, a.n - first) + 3) / 4;
+            float* dst = blkSmem + h * kBlkPart;
+            for (uint32_t i = tid; i < chunks; i += kBlkThreads) cpAsync16(dst + 4 * i, contrib + first + 4 * i);
+            cpAsyncCommit();
+        };
+        // this thread's first kBlkEdgeRegs words of tile (k, p)
+        auto loadEdges = [&](uint32_t p, uint4 (&e)[kBlkEdgeRegs], uint32_t& w0, uint32_t& w1) {
+            const uint64_t g = (uint64_t)k * b.nParts + p;
+            w0 = b.off[g];
+            w1 = b.off[g + 1];
 #pragma unroll
-                        for (int d = 1; d < 32; d <<= 1) {  // sums of equal-row runs (rows ascend along the lanes)
-                            const float v2 = __shfl_up_sync(kFull, val, d);
-                            const uint32_t r2 = __shfl_up_sync(kFull, row, d);
-                            if ((int)lane >= d && r2 == row) val += v2;
-                        }
-                        if (real && runEnd) sums[row] += val;
-                    }
-                    __syncwarp();
-                }
-                if (lane == 0)
-                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(&emptyBar[s])) : "memory");
+            for (int q = 0; q < kBlkEdgeRegs; ++q) {
+                const uint32_t i = w0 + tid + q * kBlkThreads;
+                e[q] = i < w1 ? ldStream16(b.edges + i) : make_uint4(~0u, ~0u, ~0u, ~0u);
             }
-            if (!ok) break;
-            for (uint32_t i = lo + lane; i < hi; i += 32) {
-                const uint32_t v = r0 + i;
-                if (a.rp[v + 1] - a.rp[v] >= kBlkHub) continue;
-                storeJacobi(a, cur, withDelta, v, prValue(a, sums[i], dang), acc);
+        };
+        uint4 e[kBlkEdgeRegs];
+        uint32_t w0, w1;
+        stage(partAt(0), 0);
+        loadEdges(partAt(0), e, w0, w1);
+        for (uint32_t j = 0; j < b.nParts; ++j) {
+            cpAsyncWaitAll();
+            // part j is staged by every thread, and every thread is done with part j - 1
+            __syncthreads();
+            uint4 en[kBlkEdgeRegs];
+            uint32_t n0 = 0, n1 = 0;
+            if (j + 1 < b.nParts) {
+                stage(partAt(j + 1), (j + 1) & 1u);
+                loadEdges(partAt(j + 1), en, n0, n1);
             }
-            __syncwarp();
+            const float* part = blkSmem + (j & 1u) * kBlkPart;
+#pragma unroll
+            for (int q = 0; q < kBlkEdgeRegs; ++q) blkAdd(sums, part, e[q]);
+            for (uint32_t i = w0 + tid + kBlkEdgeRegs * kBlkThreads; i < w1; i += kBlkThreads)
+                blkAdd(sums, part, ldStream16(b.edges + i));
+#pragma unroll
+            for (int q = 0; q < kBlkEdgeRegs; ++q) e[q] = en[q];
+            w0 = n0;
+            w1 = n1;
         }
-        if (!ok && lane == 0) {
-            atomicOr(&a.ctl->error, 1);
-            sErr = 1;
+        __syncthreads();
+        for (uint32_t i = tid; i < rows; i += kBlkThreads) {
+            const uint32_t v = r0 + i;
+            if (a.rp[v + 1] - a.rp[v] >= kBlkHub) continue;
+            storeJacobi(a, cur, withDelta, v, prValue(a, sums[i], dang), acc);
         }
+        __syncthreads();  // the next row block zeroes the sums
     }
-    __syncthreads();
-    if (sErr) return;
     // rows with kBlkHub or more in-edges: one block each
     __shared__ float hubHi[kBlkThreads / 32], hubLo[kBlkThreads / 32];
     for (uint32_t h = blockIdx.x; h < b.nHubs; h += gridDim.x) {
@@ -917,7 +841,7 @@ uint32_t residentGrid(K kernel, uint64_t work, uint32_t threads) {
 // the opt-in limit is raised once per process.
 static size_t blkSmemBytes() {
     static const size_t bytes = [] {
-        const size_t b = ((size_t)kBlkStages * (kBlkPart + kBlkEdgeBuf) + kBlkRowCap) * sizeof(float);
+        const size_t b = ((size_t)2 * kBlkPart + kBlkRowCap) * sizeof(float);
         GB_CUDA(cudaFuncSetAttribute(prBlockedKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b));
         return b;
     }();
@@ -943,10 +867,11 @@ static void enqueueIteration(gb_pr& h, int v, const gb_pr_options& o, PrArgs& a,
     } else if (v == GB_PR_PULL_F64) {
         prPullF64Kernel<<<gridFor(h.n * 32, tg), tg, 0, s>>>(a);
     } else if (v == GB_PR_PULL_BLOCKED) {
-        BlkArgs b{h.blkEdges.get(), h.blkOff.get(), h.blkHubs.get(), h.nRowBlocks, h.rowsPer, h.nParts, h.nBlkHubs,
-                  1ull << 22};
-        prBlockedKernel<<<(uint32_t)std::min<uint64_t>(deviceSmCount(), kMaxGrid), kBlkThreads, blkSmemBytes(), s>>>(
-            a, b);
+        BlkArgs b{reinterpret_cast<const uint4*>(h.blkEdges.get()), h.blkOff.get(), h.blkHubs.get(), h.nRowBlocks,
+                  h.rowsPer, h.nParts, h.nBlkHubs};
+        const uint32_t grid = (uint32_t)std::min<uint64_t>({(uint64_t)deviceSmCount(), (uint64_t)kMaxGrid,
+                                                            (uint64_t)std::max(h.nRowBlocks, h.nBlkHubs)});
+        prBlockedKernel<<<std::max(grid, 1u), kBlkThreads, blkSmemBytes(), s>>>(a, b);
     } else if (!inplace) {
         if (v == GB_PR_PULL_SCALAR) prPullKernel<0, false><<<pullGrid(0), tg, 0, s>>>(a);
         else if (v == GB_PR_PULL_VECTOR) prPullKernel<1, false><<<pullGrid(1), tg, 0, s>>>(a);

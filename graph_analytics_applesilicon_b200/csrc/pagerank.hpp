@@ -37,18 +37,15 @@ struct GbPrControl {
 };
 
 // Blocked pull (GB_PR_PULL_BLOCKED): rows in blocks of at most kBlkRowCap
-// (their sums in shared memory), columns in parts of kBlkPart vertices; per
-// part, its contributions and the row block's edge group (a kBlkHdr-word
-// header of per-warp ranges, then the edges) are staged in shared memory by a
-// ring of kBlkStages buffers (groups longer than kBlkEdgeBuf words read the
-// rest from global memory).  kBlkWarps consumer warps own the row block's
-// rows in kBlkWarps contiguous slices.
-constexpr uint32_t kBlkPart = 8192;
-constexpr uint32_t kBlkEdgeBuf = 8192;
-constexpr uint32_t kBlkStages = 2;
-constexpr uint32_t kBlkRowCap = 23000;
-constexpr uint32_t kBlkWarps = 31;
-constexpr uint32_t kBlkHdr = 32;
+// (their sums in shared memory, one CUDA block per row block), columns in
+// parts of kBlkPart vertices (their contributions staged in shared memory,
+// two parts at a time); tile (row block, part) holds that block's edges from
+// that part as packed 32-bit words.  Each thread prefetches kBlkEdgeRegs
+// 16-byte words of the next tile.  Rows with kBlkHub or more in-edges are
+// summed apart.
+constexpr uint32_t kBlkPart = 16384;
+constexpr uint32_t kBlkRowCap = 21504;
+constexpr int kBlkEdgeRegs = 3;
 constexpr uint32_t kBlkHub = 4096;  // rows with this many in-edges are summed apart, one block each
 constexpr int kBlkThreads = 1024;
 
@@ -106,7 +103,8 @@ struct gb_pr {
     int lastVariant = -1;
 
     // blocked pull: packed (row in block << 16 | column in part) per edge,
-    // grouped by row block then part; blkOff[k * nParts + p] starts the group
+    // grouped by row block then part; blkOff[k * nParts + p] starts tile
+    // (k, p), in 16-byte words
     gb::DevBuf<uint32_t> blkEdges, blkOff, blkHubs;
     uint32_t nRowBlocks = 0, rowsPer = 0, nParts = 0, nBlkHubs = 0;
     bool blkReady = false;

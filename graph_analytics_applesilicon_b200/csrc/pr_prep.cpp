@@ -313,19 +313,16 @@ void gb_pr::prepareGS(uint32_t pairMaxOutdeg) {
 
 // Blocked pull layout.  Row block k holds rows [k * rowsPer, (k + 1) * rowsPer)
 // (ids as given, so blocks get near-equal edge counts on graphs without
-// locality), with rowsPer <= kBlkRowCap and at least one block per SM; part p
-// holds columns [p * kBlkPart, (p + 1) * kBlkPart).  Every edge u -> v of a
-// row v with fewer than kBlkHub in-edges is stored once, as
-// (v - first row of its block) << 16 | (u - first column of its part), in the
-// group (block of v, part of u); within a group edges are in row order.  A
-// group is a kBlkHdr-word header followed by its edges, padded with
-// 0xFFFFFFFF to a multiple of 4 words (every group starts on a 16-byte
-// boundary, as bulk copies need): header word w < kBlkWarps is the index of
-// the first edge of consumer warp w's rows (rows [ceil(w R / W),
-// ceil((w + 1) R / W)) of the block, R = rowsPer, W = kBlkWarps), word
-// kBlkWarps the edge count.  Rows with kBlkHub or more in-edges are listed
-// apart (blkHubs) and summed by a whole CUDA block each, with compensated
-// sums.
+// locality), with rowsPer <= kBlkRowCap and no more row blocks than SMs when
+// the cap allows (every block then runs in one wave); part p holds columns
+// [p * kBlkPart, (p + 1) * kBlkPart).  Every edge u -> v of a row v with
+// fewer than kBlkHub in-edges is stored once, as
+// (v - first row of its block) << 16 | (u - first column of its part), in
+// tile (block of v, part of u); within a tile edges are in row order.  Tiles
+// are padded with 0xFFFFFFFF to a multiple of 4 words, so each starts on a
+// 16-byte boundary; blkOff holds their starts in 16-byte words.  Rows with
+// kBlkHub or more in-edges are listed apart (blkHubs) and summed by a whole
+// CUDA block each, with compensated sums.
 void gb_pr::prepareBlocked() {
     if (blkReady) return;
     const uint32_t* rp = hostRowIn.data();
@@ -336,56 +333,41 @@ void gb_pr::prepareBlocked() {
     rowsPer = (uint32_t)((n + nRowBlocks - 1) / nRowBlocks);
     nRowBlocks = (uint32_t)std::max<uint64_t>(1, (n + rowsPer - 1) / rowsPer);
     nParts = (uint32_t)std::max<uint64_t>(1, (n + kBlkPart - 1) / kBlkPart);
-    const uint64_t groups = (uint64_t)nRowBlocks * nParts;
-    const uint64_t R = rowsPer;
-    auto warpOf = [&](uint64_t rowLocal) { return (uint32_t)(rowLocal * kBlkWarps / R); };
+    const uint64_t tiles = (uint64_t)nRowBlocks * nParts;
     std::vector<uint32_t> hubs;
     for (uint64_t v = 0; v < n; ++v)
         if (rp[v + 1] - rp[v] >= kBlkHub) hubs.push_back((uint32_t)v);
-    // per (group, warp) edge counts, then group offsets, then headers and edges
-    std::vector<uint32_t> cnt(groups * kBlkWarps, 0);
+    // per tile edge counts, then tile offsets, then the edges
+    std::vector<uint32_t> cnt(tiles, 0);
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t k = 0; k < (int64_t)nRowBlocks; ++k) {
         const uint64_t r0 = (uint64_t)k * rowsPer, r1 = std::min<uint64_t>(n, r0 + rowsPer);
-        uint32_t* c = cnt.data() + (uint64_t)k * nParts * kBlkWarps;
+        uint32_t* c = cnt.data() + (uint64_t)k * nParts;
         for (uint64_t v = r0; v < r1; ++v) {
             if (rp[v + 1] - rp[v] >= kBlkHub) continue;
-            const uint32_t w = warpOf(v - r0);
-            for (uint32_t e = rp[v]; e < rp[v + 1]; ++e) ++c[(uint64_t)(ci[e] / kBlkPart) * kBlkWarps + w];
+            for (uint32_t e = rp[v]; e < rp[v + 1]; ++e) ++c[ci[e] / kBlkPart];
         }
     }
-    std::vector<uint32_t> off(groups + 1);
-    uint64_t total = 0;
-    for (uint64_t g = 0; g < groups; ++g) {
-        uint64_t e = 0;
-        for (uint32_t w = 0; w < kBlkWarps; ++w) e += cnt[g * kBlkWarps + w];
+    std::vector<uint32_t> off(tiles + 1);
+    uint64_t total = 0;  // 16-byte words
+    for (uint64_t g = 0; g < tiles; ++g) {
         off[g] = (uint32_t)total;
-        total += kBlkHdr + ((e + 3) & ~3ull);
-        if (total >= (1ull << 32)) throw Error(GB_ERR_ARG, "blocked pull: layout exceeds 2^32 words");
+        total += (cnt[g] + 3) / 4;
+        if (total >= (1ull << 32)) throw Error(GB_ERR_ARG, "blocked pull: layout exceeds 2^32 16-byte words");
     }
-    off[groups] = (uint32_t)total;
-    std::vector<uint32_t> packed(total, 0xFFFFFFFFu);
+    off[tiles] = (uint32_t)total;
+    std::vector<uint32_t> packed(4 * total, 0xFFFFFFFFu);
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t k = 0; k < (int64_t)nRowBlocks; ++k) {
         const uint64_t r0 = (uint64_t)k * rowsPer, r1 = std::min<uint64_t>(n, r0 + rowsPer);
-        std::vector<uint32_t> pos((uint64_t)nParts * kBlkWarps);  // next edge slot per (part, warp)
-        for (uint32_t p = 0; p < nParts; ++p) {
-            const uint64_t g = (uint64_t)k * nParts + p;
-            uint32_t* hdr = packed.data() + off[g];
-            uint32_t run = 0;
-            for (uint32_t w = 0; w < kBlkWarps; ++w) {
-                hdr[w] = run;
-                pos[(uint64_t)p * kBlkWarps + w] = off[g] + kBlkHdr + run;
-                run += cnt[g * kBlkWarps + w];
-            }
-            hdr[kBlkWarps] = run;
-        }
+        std::vector<uint64_t> pos(nParts);  // next word per part
+        for (uint32_t p = 0; p < nParts; ++p) pos[p] = 4ull * off[(uint64_t)k * nParts + p];
         for (uint64_t v = r0; v < r1; ++v) {
             if (rp[v + 1] - rp[v] >= kBlkHub) continue;
-            const uint32_t rowLocal = (uint32_t)(v - r0), w = warpOf(rowLocal);
+            const uint32_t rowLocal = (uint32_t)(v - r0);
             for (uint32_t e = rp[v]; e < rp[v + 1]; ++e) {
                 const uint32_t u = ci[e], p = u / kBlkPart;
-                packed[pos[(uint64_t)p * kBlkWarps + w]++] = rowLocal << 16 | (u - p * kBlkPart);
+                packed[pos[p]++] = rowLocal << 16 | (u - p * kBlkPart);
             }
         }
     }

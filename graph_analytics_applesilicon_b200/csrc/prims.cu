@@ -10,6 +10,8 @@
 // warp-aggregated appends.
 #include "prims.cuh"
 
+#include <cuda.h>
+
 #include <mutex>
 #include <string>
 
@@ -274,8 +276,12 @@ void fillU32(uint32_t* p, uint32_t value, uint64_t n, cudaStream_t st) {
 //    overlap on the same GPU (different streams, or host threads) race on it
 //    and both results are undefined.  Order them on one stream or with events.
 //  * The first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress, once per device, with that device current); make
-//    that first call before any stream capture begins.
+//    (cudaGetSymbolAddress, with that device current); make that first call
+//    before any stream capture begins.  The address is remembered per device
+//    together with the driver's unique id of the context it was found in: a
+//    call under another context of that device (after cudaDeviceReset, or
+//    under a context the caller created) looks the address up again, since
+//    the module, and so the array, may then sit elsewhere.
 // ------------------------------------------------------------------------
 // [0, 4096): per-tile look-back status words; [4096]: tile ticket (low 32
 // bits) and timeout flag (high 32 bits).  32 KiB + 8 bytes per device.
@@ -292,22 +298,54 @@ constexpr int kNoAllocMaxDevices = 64;
 
 std::mutex gNoAllocMu;
 unsigned long long* gNoAllocScratchPtr[kNoAllocMaxDevices] = {};
+unsigned long long gNoAllocCtxId[kNoAllocMaxDevices] = {};
+
+// The driver's unique id of the calling thread's current context (ids are
+// never reused within a process), or 0 when there is none yet or the driver
+// cannot tell.  The two driver calls are reached through the runtime's entry
+// point table, so the library needs no link against the driver library.
+unsigned long long currentContextId() {
+    struct Fns {
+        CUresult (*current)(CUcontext*) = nullptr;
+        CUresult (*id)(CUcontext, unsigned long long*) = nullptr;
+    };
+    static const Fns f = [] {
+        Fns r;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            r.current = reinterpret_cast<CUresult (*)(CUcontext*)>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            r.id = reinterpret_cast<CUresult (*)(CUcontext, unsigned long long*)>(p);
+        return r;
+    }();
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (f.current && f.id && f.current(&c) == CUDA_SUCCESS && c && f.id(c, &id) == CUDA_SUCCESS) return id;
+    return 0;
+}
 
 // Device address of the scratch array on the current device; looked up on
-// the first call for that device and remembered.
+// the first call for that device and again whenever the current context of
+// that device is not the one the address was found in.
 unsigned long long* noAllocScanScratch() {
     int dev = 0;
     GB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices)
         throw Error(GB_ERR_ARG, "no-allocation scan supports device ordinals below 64");
     std::lock_guard<std::mutex> lock(gNoAllocMu);
-    if (!gNoAllocScratchPtr[dev]) {
+    const unsigned long long ctx = currentContextId();
+    if (!gNoAllocScratchPtr[dev] || ctx == 0 || ctx != gNoAllocCtxId[dev]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, gNoAllocScanScratch);
         if (e != cudaSuccess || !p)
             throw Error(GB_ERR_CUDA, std::string("cudaGetSymbolAddress(scan scratch) failed: ") +
                                          cudaGetErrorString(e));
         gNoAllocScratchPtr[dev] = static_cast<unsigned long long*>(p);
+        gNoAllocCtxId[dev] = currentContextId();  // the lookup made the context current if none was
     }
     return gNoAllocScratchPtr[dev];
 }

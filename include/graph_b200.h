@@ -393,7 +393,9 @@ int gb_prim_scan(const uint32_t* in, uint64_t n, uint32_t* out, uint32_t* total)
  * call before its kernel; calls whose kernels overlap on the same GPU (other
  * streams, other host threads) race on it and give undefined results, so
  * order them.  The first call on each device looks up that array's address
- * with the device current; make it before any stream capture begins. */
+ * with the device current; make it before any stream capture begins.  A call
+ * under a different context of that device (after cudaDeviceReset, or under a
+ * context the caller created) looks the address up again. */
 int gb_prim_scan_device_noalloc(const uint32_t* in, uint64_t n, uint32_t* out, uint32_t* total,
                                 uint32_t* timeout_flag, void* stream);
 int gb_prim_reduce(const uint32_t* in, uint64_t n, uint32_t* sum, uint32_t* max);
