@@ -422,8 +422,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
     unsigned* bar = &a.ctl[0];
     unsigned* err = &a.ctl[1];
     const bool learned = a.selector == GB_SELECT_LEARNED && a.sel != nullptr;
-    if (learned)
-        selectorStage(sm.sel, a.sel, tid, NT);
+    // the selector's parameters arrive in shared memory while the prologue
+    // runs; the wait sits before the prologue's grid barrier (whose block
+    // barrier makes them visible to every warp)
+    if (learned) selectorStageAsync(sm.sel, a.sel, tid, NT);
 
     uint32_t level;
     bool bottomUp, qValid;
@@ -466,6 +468,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
                 c.qtail = 1;
             }
         }
+        if (learned) selectorStageWait();
         if (!gridBarrier(bar, err, a.spinLimit)) return;
         level = 0;
         bottomUp = false;
@@ -484,6 +487,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
         reached = (uint64_t)a.state[S_REACHED];
         qValid = a.state[S_QVALID] != 0;
         lastStrat = (int)a.state[S_LAST];
+        if (learned) selectorStageWait();
         if (!gridBarrier(bar, err, a.spinLimit)) return;
     }
     const uint32_t endLevel = a.maxLevels ? a.startLevel + a.maxLevels : 0xFFFFFFFFu;
@@ -524,8 +528,13 @@ __global__ void __launch_bounds__(NT, 1024 / NT) persistentBfsKernel(PArgs a) {
         // (a road graph's 1,800) then skip the evaluation.
         // A frontier of at most 32 vertices runs the rule's top-down (its hubs
         // are split by edges): every strategy costs about the same there, so
-        // the selector's evaluation would only add to the level.
-        bool useSel = a.force < 0 && learned && !(size <= 32 && !bottomUp);
+        // the selector's evaluation would only add to the level.  The MLP is
+        // evaluated only on levels the rule runs top-down (it picks the
+        // top-down strategy and may go bottom-up early, within the trust
+        // region); a bottom-up phase and its end follow the rule, where the
+        // MLP never departed from it on the benchmark graphs and its
+        // evaluation cost about 1 us per level.
+        bool useSel = a.force < 0 && learned && !bottomUp && size > 32;
         if (useSel) {
             const float lf = log2f(1.0f + (float)size), le = log2f(1.0f + (float)fedges);
             if (selLast >= 0 && bottomUp == selLastBU && fabsf(lf - selLastF) < 0.25f && fabsf(le - selLastE) < 0.25f) {

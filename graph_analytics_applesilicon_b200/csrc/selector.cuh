@@ -64,6 +64,33 @@ __device__ __forceinline__ void selectorStage(float* S, const float* P, unsigned
     }
 }
 
+// The same copy issued as asynchronous 4-byte copies (cp.async), so the
+// threads go on with other work while the parameters arrive; the caller waits
+// with selectorStageWait (each thread for its own copies) and a block barrier
+// before the first evaluation.
+__device__ __forceinline__ void selectorStageAsync(float* S, const float* P, unsigned tid, unsigned nthreads) {
+    constexpr int oW1 = 0, oB1 = oW1 + kSelHidden * kSelFeatures, oW2 = oB1 + kSelHidden,
+                  oB2 = oW2 + kSelHidden * kSelHidden, oW3 = oB2 + kSelHidden, oB3 = oW3 + kSelOutputs * kSelHidden;
+    for (unsigned i = tid; i < (unsigned)kSelParams; i += nthreads) {
+        unsigned dst = i;
+        if (i < (unsigned)oB1) {
+            const unsigned j = i / kSelFeatures, k = i % kSelFeatures;
+            dst = oW1 + k * kSelHidden + j;
+        } else if (i >= (unsigned)oW2 && i < (unsigned)oB2) {
+            const unsigned r = i - oW2, j = r / kSelHidden, k = r % kSelHidden;
+            dst = oW2 + k * kSelHidden + j;
+        } else if (i >= (unsigned)oW3 && i < (unsigned)oB3) {
+            const unsigned r = i - oW3, o = r / kSelHidden, k = r % kSelHidden;
+            dst = oW3 + k * kSelOutputs + o;
+        }
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(S + dst)),
+                     "l"(P + i)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void selectorStageWait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // One warp evaluates the MLP (lane j owns hidden unit j) on the features of
 // a level and returns the strategy to run, or -1 if an output is not finite.
 // ruleBU is the alpha/beta rule's direction; with margin 0 (and mayGoBU) the
