@@ -395,18 +395,6 @@ __device__ __forceinline__ void chunkTask(const PrArgs& a, uint32_t t, const flo
     }
 }
 
-__device__ __forceinline__ float blockSum(float x, float* sm) {
-    x = warpSum(x);
-    const unsigned lane = laneId(), wid = threadIdx.x >> 5;
-    if (lane == 0) sm[wid] = x;
-    __syncthreads();
-    float t = 0;
-    if (threadIdx.x == 0)
-        for (unsigned w = 0; w < (blockDim.x >> 5); ++w) t += sm[w];
-    __syncthreads();
-    return t;  // meaningful in thread 0
-}
-
 // Jacobi pull iteration.  MODE 0: thread per vertex (gpu_pull_scalar);
 // 1: warp per vertex (gpu_pull_vector); 2: degree-adaptive over the three
 // in-degree bins in one launch (block per large, warp per medium, thread per
@@ -416,7 +404,6 @@ __device__ __forceinline__ float blockSum(float x, float* sm) {
 // contribution, sum and scale kernels.
 template <int MODE, bool INPLACE>
 __global__ void prPullKernel(PrArgs a) {
-    __shared__ float sRed[32];
     const GbPrControl* c = a.ctl;
     if (ldvi(&c->stopped)) return;
     const int cur = c->cur;
