@@ -261,16 +261,17 @@ def max_over_ranks(vals, world):
 
 def measured_traffic(kernel, workload, grid_blocks):
     """DRAM bytes (read + write) per launch of `kernel` on `workload` at a grid of
-    `grid_blocks` blocks (None: any), as measured by ncu and recorded in
-    profiles/roofline_traffic.txt; None when no capture of that launch shape
-    is recorded."""
+    `grid_blocks` blocks (None: any; the file lists the option values that give
+    the captured grid, 0 being every resident block), as measured by ncu and
+    recorded in profiles/roofline_traffic.txt; None when no capture of that
+    launch shape is recorded."""
     try:
         with open(os.path.join(ROOT, "profiles", "roofline_traffic.txt")) as f:
             for line in f:
                 parts = line.split()
                 if line.startswith("#") or len(parts) < 4 or parts[0] != kernel or parts[1] != workload:
                     continue
-                if grid_blocks is None or parts[2] in ("*", str(grid_blocks)):
+                if grid_blocks is None or parts[2] == "*" or str(grid_blocks) in parts[2].split(","):
                     return int(parts[3])
     except OSError:
         pass
