@@ -320,12 +320,6 @@ __device__ __forceinline__ uint32_t buScanFrom(const PArgs& a, const uint32_t* f
 // after another; a vertex whose first entry is not a parent (rare once lists
 // are hub-first) continues with buScanFrom.
 constexpr int kBuWords = 4;
-// Lists with more than kBuCoop entries left after the first are scanned by
-// the whole warp.
-#ifndef GB_BU_COOP
-#define GB_BU_COOP 32
-#endif
-constexpr uint32_t kBuCoop = GB_BU_COOP;
 
 __device__ void buLevel(const PArgs& a, uint32_t level, Acc& acc) {
     const uint32_t* front = a.bm[level % 3];
@@ -360,40 +354,7 @@ __device__ void buLevel(const PArgs& a, uint32_t level, Acc& acc) {
         }
 #pragma unroll
         for (int k = 0; k < kBuWords; ++k) {
-            // the rest of each unresolved list: a short one by its own lane
-            // (buScanFrom, 4 entries per step); one of more than kBuCoop
-            // entries by the whole warp, one vertex at a time, 32 entries per
-            // step (one coalesced read, then each lane's frontier bit; the
-            // first hit by ballot) -- so a warp no longer waits for its
-            // longest list at 4 entries per step.  Both count the entries up
-            // to the first hit, as the serial scan of cpu_do does.
-            const bool coop = need[k] && !found[k] && b[k] + 1 < e[k] && e[k] - b[k] - 1 > kBuCoop;
-            if (need[k] && !found[k] && !coop)
-                acc.exam += (b[k] < e[k] ? buScanFrom(a, front, b[k] + 1, e[k], found[k]) : e[k]) - b[k];
-            for (unsigned L = __ballot_sync(kFull, coop); L; L &= L - 1) {
-                const unsigned src = __ffs(L) - 1;
-                const uint32_t lb = __shfl_sync(kFull, b[k] + 1, src), le = __shfl_sync(kFull, e[k], src);
-                bool hitAny = false;
-                uint32_t stop = le;  // one past the first hit, or the end of the list
-                for (uint32_t i = lb; i < le; i += 32) {  // warp-uniform bounds
-                    const uint32_t j = i + lane;
-                    bool h = false;
-                    if (j < le) {
-                        const uint32_t x = a.col_idx[j];
-                        h = (front[x >> 5] >> (x & 31)) & 1u;
-                    }
-                    const unsigned H = __ballot_sync(kFull, h);
-                    if (H) {
-                        hitAny = true;
-                        stop = i + __ffs(H);
-                        break;
-                    }
-                }
-                if (lane == src) {
-                    found[k] = hitAny;
-                    acc.exam += stop - b[k];
-                }
-            }
+            if (need[k] && !found[k]) acc.exam += (b[k] < e[k] ? buScanFrom(a, front, b[k] + 1, e[k], found[k]) : e[k]) - b[k];
             const unsigned F = __ballot_sync(kFull, found[k]);
             const uint64_t w = w0 + (uint64_t)k * nwarps;
             if (found[k]) {
