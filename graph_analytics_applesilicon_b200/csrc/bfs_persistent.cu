@@ -319,7 +319,10 @@ __device__ __forceinline__ uint32_t buScanFrom(const PArgs& a, const uint32_t* f
 // four dependent loads of the words overlap instead of running one word
 // after another; a vertex whose first entry is not a parent (rare once lists
 // are hub-first) continues with buScanFrom.
-constexpr int kBuWords = 4;
+#ifndef GB_BU_WORDS
+#define GB_BU_WORDS 4
+#endif
+constexpr int kBuWords = GB_BU_WORDS;
 
 __device__ void buLevel(const PArgs& a, uint32_t level, Acc& acc) {
     const uint32_t* front = a.bm[level % 3];
