@@ -333,45 +333,6 @@ __device__ __forceinline__ float gatherGroup(const uint32_t* __restrict__ ci, co
     return k.sum;
 }
 
-// gatherGroup with the index loads one step ahead: the 16-byte index vectors
-// of step s + 1 are requested before the gathers of step s, so a step waits
-// for one round trip (its gathers) instead of two (indices, then gathers).
-// Same per-lane order of additions as gatherGroup.
-template <bool COHERENT>
-__device__ __forceinline__ float gatherGroupPipelined(const uint32_t* __restrict__ ci, const float* contrib,
-                                                      uint32_t b, uint32_t e, unsigned rank, unsigned G) {
-    Kahan k;
-    const uint32_t step = 4 * G;
-    const uint4 zero = make_uint4(0, 0, 0, 0);
-    uint32_t i = (b & ~3u) + 4 * rank;
-    uint4 q = i < e ? ldStream4(ci + i) : zero;
-    uint4 r = i + step < e ? ldStream4(ci + i + step) : zero;
-    for (; i < e; i += 2 * step) {
-        const uint32_t j = i + step, i2 = i + 2 * step;
-        const uint4 qn = i2 < e ? ldStream4(ci + i2) : zero;
-        const uint4 rn = i2 + step < e ? ldStream4(ci + i2 + step) : zero;
-        const float a0 = (i >= b) ? ldContrib<COHERENT>(contrib + q.x) : 0.f;
-        const float a1 = (i + 1 >= b && i + 1 < e) ? ldContrib<COHERENT>(contrib + q.y) : 0.f;
-        const float a2 = (i + 2 >= b && i + 2 < e) ? ldContrib<COHERENT>(contrib + q.z) : 0.f;
-        const float a3 = (i + 3 >= b && i + 3 < e) ? ldContrib<COHERENT>(contrib + q.w) : 0.f;
-        const float b0 = (j < e) ? ldContrib<COHERENT>(contrib + r.x) : 0.f;
-        const float b1 = (j + 1 < e) ? ldContrib<COHERENT>(contrib + r.y) : 0.f;
-        const float b2 = (j + 2 < e) ? ldContrib<COHERENT>(contrib + r.z) : 0.f;
-        const float b3 = (j + 3 < e) ? ldContrib<COHERENT>(contrib + r.w) : 0.f;
-        k.add(a0);
-        k.add(a1);
-        k.add(a2);
-        k.add(a3);
-        k.add(b0);
-        k.add(b1);
-        k.add(b2);
-        k.add(b3);
-        q = qn;
-        r = rn;
-    }
-    return k.sum;
-}
-
 // One warp chunk of a split vertex: the warp's sum goes to the chunk's
 // partial; the warp finishing the vertex's last chunk (ticket per vertex)
 // adds the partials in chunk order (Kahan) and stores the vertex.  All 32
@@ -440,8 +401,11 @@ __global__ void prPullKernel(PrArgs a) {
         for (int b = 0; b < a.nBins; ++b) total += ((uint64_t)(a.binHi[b] - a.binLo[b]) * a.binG[b] + 31) / 32;
         const uint64_t nwarps = gthreads >> 5;
         const unsigned lane = laneId();
-        // a degree-class task t: its group size and this lane's vertex
-        auto taskOf = [&](uint64_t t, unsigned& G, uint32_t& v, bool& active) {
+        for (uint64_t t = gtid >> 5; t < total; t += nwarps) {  // warp-uniform
+            if (t < a.nChunks) {
+                chunkTask<INPLACE>(a, (uint32_t)t, contrib, store);
+                continue;
+            }
             uint64_t tb = t - a.nChunks;
             int b = 0;
             for (; b < a.nBins; ++b) {
@@ -449,40 +413,12 @@ __global__ void prPullKernel(PrArgs a) {
                 if (tb < nt) break;
                 tb -= nt;
             }
-            G = a.binG[b];
-            v = a.binLo[b] + (uint32_t)tb * (32 / G) + lane / G;
-            active = v < a.binHi[b];
-        };
-        uint64_t t = gtid >> 5;
-        for (; t < total && t < a.nChunks; t += nwarps)  // warp-uniform
-            chunkTask<INPLACE>(a, (uint32_t)t, contrib, store);
-        // degree-class tasks: the next task's row bounds are requested before
-        // this task's gathers
-        unsigned G = 1;
-        uint32_t v = 0, rb = 0, re = 0;
-        bool active = false;
-        if (t < total) {
-            taskOf(t, G, v, active);
-            rb = active ? a.rp[v] : 0u;
-            re = active ? a.rp[v + 1] : 0u;
-        }
-        for (; t < total; t += nwarps) {  // warp-uniform
-            unsigned G2 = 1;
-            uint32_t v2 = 0, rb2 = 0, re2 = 0;
-            bool active2 = false;
-            if (t + nwarps < total) {
-                taskOf(t + nwarps, G2, v2, active2);
-                rb2 = active2 ? a.rp[v2] : 0u;
-                re2 = active2 ? a.rp[v2 + 1] : 0u;
-            }
-            float s = active ? gatherGroupPipelined<INPLACE>(a.ci, contrib, rb, re, lane & (G - 1), G) : 0.f;
+            const unsigned G = a.binG[b];
+            const uint32_t v = a.binLo[b] + (uint32_t)tb * (32 / G) + lane / G;
+            const bool active = v < a.binHi[b];
+            float s = active ? gatherGroup<INPLACE>(a.ci, contrib, a.rp[v], a.rp[v + 1], lane & (G - 1), G) : 0.f;
             for (unsigned o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
             if (active && (lane & (G - 1)) == 0) store(v, s);
-            G = G2;
-            v = v2;
-            rb = rb2;
-            re = re2;
-            active = active2;
         }
     }
     if (!INPLACE) finishBlock<0>(a, acc);
