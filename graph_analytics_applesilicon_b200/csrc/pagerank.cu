@@ -584,30 +584,42 @@ __global__ void prPushFinalizeKernel(PrArgs a) {
 // block of kBlkThreads per row block (one per SM at the graph sizes this form
 // is for), looping over the column parts starting at a part that depends on
 // the row block (the SMs then stage different contributions at once).  Part
-// j + 1's contributions are copied into the other half of a two-part ring by
-// cp.async while part j's edges are summed, and every thread holds the first
+// j + 1's contributions arrive in the other half of a two-part ring by one
+// TMA bulk copy (cp.async.bulk, completion counted on that half's mbarrier)
+// while part j's edges are summed, and every thread holds the first
 // kBlkEdgeRegs 16-byte words of its share of part j + 1's edges in registers
-// by then, so one block barrier per part separates the parts and the copies
-// and loads of the next part overlap this part's work.  Every thread takes
-// an equal share of each tile's edges (no row ownership, so no warp waits for
-// another's heavier rows).  Rows with kBlkHub or more in-edges are summed
-// afterwards by one block each with Kahan-compensated per-thread sums
-// combined as float-float; the other rows' sums are plain FP32 (fewer than
-// kBlkHub terms).
+// by then; one block barrier per part frees the ring half for the next copy.
+// Every thread takes an equal share of each tile's edges (no row ownership,
+// so no warp waits for another's heavier rows).  Rows with kBlkHub or more
+// in-edges are summed afterwards by one block each with Kahan-compensated
+// per-thread sums combined as float-float; the other rows' sums are plain
+// FP32 (fewer than kBlkHub terms).  Every mbarrier wait is bounded: on a
+// timeout the block records the error in the control block, waits (bounded)
+// for its copy in flight and leaves without storing.
 struct BlkArgs {
     const uint4* edges;     // tiles of packed (row in block << 16 | column in part) words, 0xFFFFFFFF padding
     const uint32_t* off;    // 16-byte-word offset of tile (k, p) at k * nParts + p, then the end
     const uint32_t* hubs;
     uint32_t nRowBlocks, rowsPer, nParts, nHubs;
+    unsigned long long spinLimit;
 };
 
-__device__ __forceinline__ void cpAsync16(float* dst, const float* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
-                 "l"(src)
-                 : "memory");
+__device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Waits for the given phase parity of an mbarrier; gives up after `limit` polls.
+__device__ __forceinline__ bool blkWait(unsigned long long* mbar, uint32_t parity, unsigned long long limit) {
+    const uint32_t addr = smemAddr(mbar);
+    for (unsigned long long i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
 }
-__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ uint4 ldStream16(const uint4* p) {
     uint4 v;
@@ -627,7 +639,8 @@ __device__ __forceinline__ void blkAdd(float* sums, const float* part, uint4 w) 
 
 __global__ void __launch_bounds__(kBlkThreads, 1) prBlockedKernel(PrArgs a, BlkArgs b) {
     // [0, 2 kBlkPart): the contribution ring; then the row block's sums
-    extern __shared__ __align__(16) float blkSmem[];
+    extern __shared__ __align__(128) float blkSmem[];
+    __shared__ __align__(8) unsigned long long full[2];
     const GbPrControl* c = a.ctl;
     if (ldvi(&c->stopped)) return;
     const int cur = c->cur;
@@ -636,19 +649,35 @@ __global__ void __launch_bounds__(kBlkThreads, 1) prBlockedKernel(PrArgs a, BlkA
     const float* contrib = a.contrib[cur];
     float* sums = blkSmem + 2 * kBlkPart;
     const unsigned tid = threadIdx.x;
+    if (tid == 0) {
+        for (int h = 0; h < 2; ++h)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(&full[h])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
     IterAcc acc;
-    for (uint32_t k = blockIdx.x; k < b.nRowBlocks; k += gridDim.x) {
+    uint32_t t = 0;        // parts staged so far: part t uses ring half t & 1, fill number t >> 1
+    bool failed = false;
+    for (uint32_t k = blockIdx.x; k < b.nRowBlocks && !failed; k += gridDim.x) {
         const uint32_t r0 = k * b.rowsPer, rows = min(a.n - r0, b.rowsPer);
         for (uint32_t i = tid; i < rows; i += kBlkThreads) sums[i] = 0.0f;
         const uint32_t rot = (uint32_t)((uint64_t)k * b.nParts / b.nRowBlocks);
         auto partAt = [&](uint32_t j) { return j + rot < b.nParts ? j + rot : j + rot - b.nParts; };
-        // part p's contributions into ring half h: 16-byte copies (the
-        // contribution arrays carry 4 floats of slack past n)
+        // part p's contributions into ring half h: one bulk copy of whole
+        // 16-byte groups (the contribution arrays carry 4 floats of slack past n)
         auto stage = [&](uint32_t p, uint32_t h) {
-            const uint32_t first = p * kBlkPart, chunks = (min(kBlkPart, a.n - first) + 3) / 4;
-            float* dst = blkSmem + h * kBlkPart;
-            for (uint32_t i = tid; i < chunks; i += kBlkThreads) cpAsync16(dst + 4 * i, contrib + first + 4 * i);
-            cpAsyncCommit();
+            if (tid != 0) return;
+            const uint32_t first = p * kBlkPart;
+            const uint32_t bytes = ((min(kBlkPart, a.n - first) * 4u) + 15u) & ~15u;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(&full[h])),
+                         "r"(bytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smemAddr(blkSmem + h * kBlkPart)),
+                "l"(contrib + first), "r"(bytes), "r"(smemAddr(&full[h]))
+                : "memory");
         };
         // this thread's first kBlkEdgeRegs words of tile (k, p)
         auto loadEdges = [&](uint32_t p, uint4 (&e)[kBlkEdgeRegs], uint32_t& w0, uint32_t& w1) {
@@ -663,19 +692,25 @@ __global__ void __launch_bounds__(kBlkThreads, 1) prBlockedKernel(PrArgs a, BlkA
         };
         uint4 e[kBlkEdgeRegs];
         uint32_t w0, w1;
-        stage(partAt(0), 0);
+        // the block barrier at the end of the previous row block (or the
+        // mbarrier set-up) has freed both ring halves
+        stage(partAt(0), t & 1u);
         loadEdges(partAt(0), e, w0, w1);
-        for (uint32_t j = 0; j < b.nParts; ++j) {
-            cpAsyncWaitAll();
-            // part j is staged by every thread, and every thread is done with part j - 1
-            __syncthreads();
+        for (uint32_t j = 0; j < b.nParts; ++j, ++t) {
+            const bool ok = blkWait(&full[t & 1u], (t >> 1) & 1u, b.spinLimit);
+            // part j is staged; every thread is done with part j - 1, whose
+            // ring half the next copy overwrites; the block agrees on a timeout
+            if (__syncthreads_or(!ok)) {
+                failed = true;
+                break;
+            }
             uint4 en[kBlkEdgeRegs];
             uint32_t n0 = 0, n1 = 0;
             if (j + 1 < b.nParts) {
-                stage(partAt(j + 1), (j + 1) & 1u);
+                stage(partAt(j + 1), (t + 1) & 1u);
                 loadEdges(partAt(j + 1), en, n0, n1);
             }
-            const float* part = blkSmem + (j & 1u) * kBlkPart;
+            const float* part = blkSmem + (t & 1u) * kBlkPart;
 #pragma unroll
             for (int q = 0; q < kBlkEdgeRegs; ++q) blkAdd(sums, part, e[q]);
             for (uint32_t i = w0 + tid + kBlkEdgeRegs * kBlkThreads; i < w1; i += kBlkThreads)
@@ -685,13 +720,24 @@ __global__ void __launch_bounds__(kBlkThreads, 1) prBlockedKernel(PrArgs a, BlkA
             w0 = n0;
             w1 = n1;
         }
+        if (failed) break;
         __syncthreads();
         for (uint32_t i = tid; i < rows; i += kBlkThreads) {
             const uint32_t v = r0 + i;
             if (a.rp[v + 1] - a.rp[v] >= kBlkHub) continue;
             storeJacobi(a, cur, withDelta, v, prValue(a, sums[i], dang), acc);
         }
-        __syncthreads();  // the next row block zeroes the sums
+        __syncthreads();  // the next row block zeroes the sums and refills the ring
+    }
+    if (failed) {
+        // the block stopped at part t before issuing the next copy, so part
+        // t's own copy is the only one that may still be landing: let it
+        // arrive (bounded) before the block's shared memory is released
+        if (tid == 0) {
+            atomicOr(&a.ctl->error, 1);
+            blkWait(&full[t & 1u], (t >> 1) & 1u, b.spinLimit);
+        }
+        return;
     }
     // rows with kBlkHub or more in-edges: one block each
     __shared__ float hubHi[kBlkThreads / 32], hubLo[kBlkThreads / 32];
@@ -715,14 +761,14 @@ __global__ void __launch_bounds__(kBlkThreads, 1) prBlockedKernel(PrArgs a, BlkA
         }
         __syncthreads();
         if (tid == 0) {
-            FF t;
+            FF t2;
             for (int w = 0; w < kBlkThreads / 32; ++w) {
                 FF x;
                 x.hi = hubHi[w];
                 x.lo = hubLo[w];
-                t.add(x);
+                t2.add(x);
             }
-            storeJacobi(a, cur, withDelta, v, prValue(a, t.hi + t.lo, dang), acc);
+            storeJacobi(a, cur, withDelta, v, prValue(a, t2.hi + t2.lo, dang), acc);
         }
         __syncthreads();
     }
@@ -855,7 +901,7 @@ static void enqueueIteration(gb_pr& h, int v, const gb_pr_options& o, PrArgs& a,
         prPullF64Kernel<<<gridFor(h.n * 32, tg), tg, 0, s>>>(a);
     } else if (v == GB_PR_PULL_BLOCKED) {
         BlkArgs b{reinterpret_cast<const uint4*>(h.blkEdges.get()), h.blkOff.get(), h.blkHubs.get(), h.nRowBlocks,
-                  h.rowsPer, h.nParts, h.nBlkHubs};
+                  h.rowsPer, h.nParts, h.nBlkHubs, 1ull << 22};
         const uint32_t grid = (uint32_t)std::min<uint64_t>({(uint64_t)deviceSmCount(), (uint64_t)kMaxGrid,
                                                             (uint64_t)std::max(h.nRowBlocks, h.nBlkHubs)});
         prBlockedKernel<<<std::max(grid, 1u), kBlkThreads, blkSmemBytes(), s>>>(a, b);
