@@ -58,7 +58,7 @@ class BfsOptions(C.Structure):
                 ("ept", C.c_uint32), ("alpha", C.c_double), ("beta", C.c_double),
                 ("selector", C.c_uint32), ("force_strategy", C.c_int32), ("hub_min", C.c_uint32),
                 ("block", C.c_uint32), ("spin_limit", C.c_uint64), ("grid_blocks", C.c_uint32),
-                ("sel_margin", C.c_float)]
+                ("sel_margin", C.c_float), ("in_flight", C.c_uint32)]
 
     def __init__(self, **kw):
         super().__init__()

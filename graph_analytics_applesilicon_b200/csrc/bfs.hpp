@@ -42,7 +42,8 @@ int packFormat(uint64_t count, uint32_t levels);
 uint64_t packedBytes(int fmt, uint64_t count);
 void enqueuePack(int fmt, const uint32_t* d, uint64_t count, uint8_t* dev, unsigned* overflow, cudaStream_t st);
 void widenPacked(int fmt, const uint8_t* in, uint64_t count, uint32_t* out);
-constexpr int kManySlots = 3;  // depth buffers in flight in gb_bfs::runPersistentMany
+constexpr int kMaxInFlight = 4;              // traversals at once in gb_bfs::runPersistentMany
+constexpr int kManySlots = kMaxInFlight + 2;  // depth buffers it rotates (in flight + 2)
 }  // namespace gb
 
 struct gb_bfs {
@@ -74,6 +75,17 @@ struct gb_bfs {
     gb::DevBuf<gb_level> ptrace;
     gb::DevBuf<double> pstate;           // level state for resumable (profiling) runs
     int pGrid = 0, pBlock = 0, pMax = 0, pWant = 0;
+    // further traversals in flight in runPersistentMany: the same per-traversal
+    // state (slot 0 is the members above) and a stream each
+    struct PSlot {
+        gb::DevBuf<uint32_t> q[2][3], hub[2][2], bm[3], visited;
+        gb::DevBuf<unsigned long long> hubOff[2];
+        gb::DevBuf<GbPCounters> ctr;
+        gb::DevBuf<gb_level> trace;
+        gb::DevBuf<double> state;
+    };
+    PSlot pSlot[gb::kMaxInFlight - 1];
+    gb::Stream pStream[gb::kMaxInFlight - 1];
 
     // batched (64 sources)
     gb::DevBuf<unsigned long long> bSeen, bFront[2], bNext;

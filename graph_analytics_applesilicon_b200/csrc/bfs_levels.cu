@@ -30,6 +30,8 @@ void validateOptions(const gb_bfs_options& o) {
     if (o.block != 0 && o.block != 256 && o.block != 512)
         throw Error(GB_ERR_ARG, "persistent block size must be 256 or 512");
     if (o.selector > GB_SELECT_LEARNED) throw Error(GB_ERR_ARG, "unknown selector");
+    if (o.in_flight > (uint32_t)kMaxInFlight)
+        throw Error(GB_ERR_ARG, "in_flight must be at most " + std::to_string(kMaxInFlight));
 }
 
 namespace {

@@ -735,9 +735,9 @@ __global__ void isolatedBitmapKernel(const uint32_t* __restrict__ row_ptr, uint6
 }
 
 template <int NT>
-void launchPersistent(gb_bfs& h, PArgs& a) {
+void launchPersistent(PArgs& a, int grid, cudaStream_t st) {
     void* args[] = {&a};
-    GB_CUDA(cudaLaunchCooperativeKernel((void*)persistentBfsKernel<NT>, dim3(h.pGrid), dim3(NT), args, 0, h.stream.s));
+    GB_CUDA(cudaLaunchCooperativeKernel((void*)persistentBfsKernel<NT>, dim3(grid), dim3(NT), args, 0, st));
 }
 
 PArgs makeArgs(gb_bfs& h, const gb_bfs_options& o, uint32_t src) {
@@ -778,9 +778,29 @@ PArgs makeArgs(gb_bfs& h, const gb_bfs_options& o, uint32_t src) {
     return a;
 }
 
-void launchFor(gb_bfs& h, PArgs& a) {
-    if (h.pBlock == 256) launchPersistent<256>(h, a);
-    else launchPersistent<512>(h, a);
+void launchFor(gb_bfs& h, PArgs& a, int grid = 0, cudaStream_t st = nullptr) {
+    if (!grid) grid = h.pGrid;
+    if (!st) st = h.stream.s;
+    if (h.pBlock == 256) launchPersistent<256>(a, grid, st);
+    else launchPersistent<512>(a, grid, st);
+}
+
+// The state of in-flight slot `slot` (> 0) in place of slot 0's.
+void useSlot(gb_bfs& h, PArgs& a, int slot) {
+    gb_bfs::PSlot& p = h.pSlot[slot - 1];
+    for (int i = 0; i < 2; ++i) {
+        a.qv[i] = p.q[i][0].get();
+        a.qs[i] = p.q[i][1].get();
+        a.qd[i] = p.q[i][2].get();
+        a.hv[i] = p.hub[i][0].get();
+        a.hs[i] = p.hub[i][1].get();
+        a.ho[i] = p.hubOff[i].get();
+    }
+    for (int i = 0; i < 3; ++i) a.bm[i] = p.bm[i].get();
+    a.visited = p.visited.get();
+    a.ctr = p.ctr.get();
+    a.trace = p.trace.get();
+    a.state = p.state.get();
 }
 
 }  // namespace
@@ -811,6 +831,19 @@ void gb_bfs::ensurePersistent(const gb_bfs_options& o) {
     pctl.ensure(4);
     ptrace.ensure(kTraceCap);
     pstate.ensure(S_COUNT);
+    for (uint32_t k = 1; k < std::max<uint32_t>(1, o.in_flight); ++k) {
+        PSlot& p = pSlot[k - 1];
+        for (int i = 0; i < 2; ++i) {
+            for (int j = 0; j < 3; ++j) p.q[i][j].ensure(n);
+            for (int j = 0; j < 2; ++j) p.hub[i][j].ensure(hubCap);
+            p.hubOff[i].ensure(hubCap);
+        }
+        for (auto& b : p.bm) b.ensure(words);
+        p.visited.ensure(words);
+        p.ctr.ensure(3);
+        p.trace.ensure(kTraceCap);
+        p.state.ensure(S_COUNT);
+    }
     if (pBlock != block) {
         int perSm = 0;
         if (block == 256)
@@ -850,16 +883,23 @@ void gb_bfs::runPersistent(uint32_t src, const gb_bfs_options& o, std::vector<gb
     }
 }
 
-// Several sources in one call.  Traversal i writes depth buffer i % kManySlots
-// (dist, then mDist[]) and its own four control words (all zeroed by one
-// memset), so the traversals follow one another on the stream with no host
-// round trip between them.  With a host output, traversal i's depths are
-// packed on the stream right behind it (the width predicted from the most
+// Several sources in one call.  K = in_flight traversals run at once:
+// traversal i runs on stream i % K (stream 0 is the handle's) with that
+// slot's state, on a cooperative grid of grid_blocks blocks (0: the resident
+// blocks / K), writing depth buffer i % B (B = K + 2: dist, then mDist[]) and
+// its own four control words (all zeroed by one memset).  The traversals of
+// one stream follow one another with no host round trip, and the K streams
+// run side by side: a traversal's levels wait on dependent loads and its grid
+// barrier, so K of them on a share of the SMs each overlap those waits.  A
+// depth buffer is refilled only after its previous traversal (and, with a host
+// output, that one's pack and copy) are done: the stream that reuses it waits
+// on the buffer's events.  With a host output, traversal i's depths are
+// packed on its stream right behind it (the width predicted from the most
 // levels seen so far; a depth that does not fit raises the overflow flag),
 // copied to pinned memory on the copy stream, and widened by host threads
 // while the next traversals run.  The host finishes source i before it queues
-// traversal i + kManySlots, the next user of slot i % kManySlots, so an
-// overflowing source can still be copied whole from its depth buffer.
+// traversal i + B, the next user of buffer i % B, so an overflowing source can
+// still be copied whole from its depth buffer.
 void gb_bfs::runPersistentMany(const uint32_t* src, uint32_t count, uint32_t* out, uint64_t stride,
                                const gb_bfs_options& o, float* msOut, uint32_t* levelsOut) {
     validateOptions(o);
@@ -867,11 +907,19 @@ void gb_bfs::runPersistentMany(const uint32_t* src, uint32_t count, uint32_t* ou
     if (o.selector == GB_SELECT_LEARNED && !selLoaded[0])
         throw Error(GB_ERR_STATE, "learned selector requested but no parameters are loaded");
     if (count == 0) return;
-    for (auto& d : mDist) d.ensure(n + 4);
-    for (int s = 0; s < kManySlots; ++s) {  // sized for the widest packed form up front
-        mPackDev[s].ensure(2 * n + 16);
-        mPackHost[s].ensure(2 * n + 16);
+    const uint32_t K = std::max<uint32_t>(1, o.in_flight), B = K + 2;
+    int grid = pGrid;
+    if (K > 1) {
+        const int share = pMax / (int)K;
+        if (share < 1) throw Error(GB_ERR_ARG, "in_flight exceeds the resident blocks of the persistent kernel");
+        grid = pWant > 0 ? std::min(pWant, share) : share;
     }
+    for (uint32_t b = 1; b < B; ++b) mDist[b - 1].ensure(n + 4);
+    if (out)
+        for (uint32_t b = 0; b < B; ++b) {  // sized for the widest packed form up front
+            mPackDev[b].ensure(2 * n + 16);
+            mPackHost[b].ensure(2 * n + 16);
+        }
     mCtl.ensure((size_t)count * 4);
     mCtlHost.ensure((size_t)count * 4);
     mFlag.ensure(kManySlots);
@@ -881,54 +929,77 @@ void gb_bfs::runPersistentMany(const uint32_t* src, uint32_t count, uint32_t* ou
         GB_CUDA(cudaEventCreate(&e));
         mEv.push_back(e);
     }
-    while (mSlotEv.size() < 2 * (size_t)kManySlots) {
+    // per buffer: packed, copied, released; then the start event and one end event per stream
+    while (mSlotEv.size() < 3 * (size_t)kManySlots + 1 + kMaxInFlight) {
         cudaEvent_t e;
         GB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         mSlotEv.push_back(e);
     }
     uint32_t* bufs[kManySlots];
     bufs[0] = dist.get();
-    for (int s = 1; s < kManySlots; ++s) bufs[s] = mDist[s - 1].get();
+    for (uint32_t b = 1; b < B; ++b) bufs[b] = mDist[b - 1].get();
+    cudaStream_t streams[kMaxInFlight];
+    streams[0] = stream.s;
+    for (uint32_t k = 1; k < K; ++k) streams[k] = pStream[k - 1].s;
+    cudaEvent_t startEv = mSlotEv[3 * kManySlots];
     std::vector<int> fmt(count, -1);
     // packed width: from the most levels among this call's finished sources,
     // else the handle's last run, else one byte per depth
     uint32_t maxSeen = 0;
     bool anySeen = false;
     const bool timed = msOut != nullptr;
-    cudaStream_t st = stream.s, cs = copyStream.s;
+    cudaStream_t cs = copyStream.s;
 
-    GB_CUDA(cudaMemsetAsync(mCtl.get(), 0, (size_t)count * 4 * sizeof(unsigned), st));
+    GB_CUDA(cudaMemsetAsync(mCtl.get(), 0, (size_t)count * 4 * sizeof(unsigned), stream.s));
+    // the other streams start after the work queued before this call on the handle's stream
+    GB_CUDA(cudaEventRecord(startEv, stream.s));
+    for (uint32_t k = 1; k < K; ++k) GB_CUDA(cudaStreamWaitEvent(streams[k], startEv, 0));
     auto enqueue = [&](uint32_t i) {
-        const int s = (int)(i % kManySlots);
+        const uint32_t k = i % K, b = i % B;
+        cudaStream_t st = streams[k];
         PArgs a = makeArgs(*this, o, src[i]);
-        a.dist = bufs[s];
+        if (k) useSlot(*this, a, (int)k);
+        a.dist = bufs[b];
         a.ctl = mCtl.get() + 4 * (size_t)i;
+        cudaEvent_t packed = mSlotEv[b], copied = mSlotEv[kManySlots + b], released = mSlotEv[2 * kManySlots + b];
+        if (i >= B) {  // buffer b's previous traversal (and its pack and copy) first
+            GB_CUDA(cudaStreamWaitEvent(st, released, 0));
+            if (out) GB_CUDA(cudaStreamWaitEvent(st, copied, 0));
+        }
         if (timed || i + 1 == count) GB_CUDA(cudaEventRecord(mEv[2 * i], st));
-        GB_CUDA(cudaMemsetAsync(bufs[s], 0xFF, n * 4, st));  // every depth infinity
-        launchFor(*this, a);
+        GB_CUDA(cudaMemsetAsync(bufs[b], 0xFF, n * 4, st));  // every depth infinity
+        launchFor(*this, a, grid, st);
         if (timed || i + 1 == count) GB_CUDA(cudaEventRecord(mEv[2 * i + 1], st));
-        if (!out) return;
-        cudaEvent_t packed = mSlotEv[s], copied = mSlotEv[kManySlots + s];
+        if (!out) {
+            GB_CUDA(cudaEventRecord(released, st));
+            return;
+        }
         fmt[i] = packFormat(n, anySeen ? maxSeen : lastLevels ? lastLevels : 254);
         if (fmt[i] >= 0) {
-            // the slot's previous copy must have left mPackDev[s]
-            if (i >= (uint32_t)kManySlots) GB_CUDA(cudaStreamWaitEvent(st, copied, 0));
-            GB_CUDA(cudaMemsetAsync(mFlag.get() + s, 0, sizeof(unsigned), st));
-            enqueuePack(fmt[i], bufs[s], n, mPackDev[s].get(), mFlag.get() + s, st);
+            GB_CUDA(cudaMemsetAsync(mFlag.get() + b, 0, sizeof(unsigned), st));
+            enqueuePack(fmt[i], bufs[b], n, mPackDev[b].get(), mFlag.get() + b, st);
         }
         GB_CUDA(cudaEventRecord(packed, st));
+        GB_CUDA(cudaEventRecord(released, st));
         GB_CUDA(cudaStreamWaitEvent(cs, packed, 0));
         if (fmt[i] >= 0) {
-            GB_CUDA(cudaMemcpyAsync(mPackHost[s].p, mPackDev[s].get(), packedBytes(fmt[i], n),
+            GB_CUDA(cudaMemcpyAsync(mPackHost[b].p, mPackDev[b].get(), packedBytes(fmt[i], n),
                                     cudaMemcpyDeviceToHost, cs));
-            GB_CUDA(cudaMemcpyAsync(mFlagHost.p + i, mFlag.get() + s, sizeof(unsigned), cudaMemcpyDeviceToHost, cs));
+            GB_CUDA(cudaMemcpyAsync(mFlagHost.p + i, mFlag.get() + b, sizeof(unsigned), cudaMemcpyDeviceToHost, cs));
         }
         GB_CUDA(cudaMemcpyAsync(mCtlHost.p + 4 * (size_t)i, mCtl.get() + 4 * (size_t)i, 4 * sizeof(unsigned),
                                 cudaMemcpyDeviceToHost, cs));
         GB_CUDA(cudaEventRecord(copied, cs));
     };
+    auto joinStreams = [&]() {  // the handle's stream covers every stream's work
+        for (uint32_t k = 1; k < K; ++k) {
+            cudaEvent_t endEv = mSlotEv[3 * kManySlots + 1 + k];
+            GB_CUDA(cudaEventRecord(endEv, streams[k]));
+            GB_CUDA(cudaStreamWaitEvent(stream.s, endEv, 0));
+        }
+    };
     auto timeout = [&]() {
-        cudaStreamSynchronize(st);
+        for (uint32_t k = 0; k < K; ++k) cudaStreamSynchronize(streams[k]);
         cudaStreamSynchronize(cs);
         return Error(GB_ERR_TIMEOUT, "persistent BFS: grid barrier wait exceeded its spin limit");
     };
@@ -936,27 +1007,29 @@ void gb_bfs::runPersistentMany(const uint32_t* src, uint32_t count, uint32_t* ou
     uint32_t queued = 0;
     if (!out) {
         for (; queued < count; ++queued) enqueue(queued);
+        joinStreams();
         GB_CUDA(cudaMemcpyAsync(mCtlHost.p, mCtl.get(), (size_t)count * 4 * sizeof(unsigned),
-                                cudaMemcpyDeviceToHost, st));
+                                cudaMemcpyDeviceToHost, stream.s));
     } else {
         for (uint32_t i = 0; i < count; ++i) {
-            for (; queued < count && queued < i + (uint32_t)kManySlots; ++queued) enqueue(queued);
-            const int s = (int)(i % kManySlots);
-            GB_CUDA(cudaEventSynchronize(mSlotEv[kManySlots + s]));
+            for (; queued < count && queued < i + B; ++queued) enqueue(queued);
+            const uint32_t b = i % B;
+            GB_CUDA(cudaEventSynchronize(mSlotEv[kManySlots + b]));
             const unsigned* c = mCtlHost.p + 4 * (size_t)i;
             if (c[1]) throw timeout();
             maxSeen = std::max(maxSeen, c[2]);
             anySeen = true;
             uint32_t* dst = out + (uint64_t)i * stride;
             if (fmt[i] >= 0 && mFlagHost.p[i] == 0) {
-                widenPacked(fmt[i], mPackHost[s].p, n, dst);
+                widenPacked(fmt[i], mPackHost[b].p, n, dst);
             } else {  // too many levels for the predicted width: the buffer is still intact
-                GB_CUDA(cudaMemcpyAsync(dst, bufs[s], n * 4, cudaMemcpyDeviceToHost, st));
-                GB_CUDA(cudaStreamSynchronize(st));
+                GB_CUDA(cudaMemcpyAsync(dst, bufs[b], n * 4, cudaMemcpyDeviceToHost, cs));
+                GB_CUDA(cudaStreamSynchronize(cs));
             }
         }
+        joinStreams();
     }
-    GB_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t k = 0; k < K; ++k) GB_CUDA(cudaStreamSynchronize(streams[k]));
     GB_CUDA(cudaStreamSynchronize(cs));
     for (uint32_t i = 0; i < count; ++i)
         if (mCtlHost.p[4 * (size_t)i + 1]) throw timeout();
@@ -968,8 +1041,8 @@ void gb_bfs::runPersistentMany(const uint32_t* src, uint32_t count, uint32_t* ou
     GB_CUDA(cudaEventElapsedTime(&last, mEv[2 * (count - 1)], mEv[2 * (count - 1) + 1]));
     lastGpuMs = last;
     lastLevels = mCtlHost.p[4 * (size_t)(count - 1) + 2];
-    const int lastSlot = (int)((count - 1) % kManySlots);
-    if (lastSlot) dist.swap(mDist[lastSlot - 1]);  // dist holds the last source's depths
+    const uint32_t lastBuf = (count - 1) % B;
+    if (lastBuf) dist.swap(mDist[lastBuf - 1]);  // dist holds the last source's depths
 }
 
 // Selector training data.  A level's vertex set does not depend on the

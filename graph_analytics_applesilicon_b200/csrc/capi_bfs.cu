@@ -197,6 +197,7 @@ void gb_bfs_default_options(gb_bfs_options* o) {
     o->spin_limit = 0;
     o->grid_blocks = 0;
     o->sel_margin = 0.5f;
+    o->in_flight = 1;
 }
 
 int gb_bfs_create(const uint32_t* row_ptr, const uint32_t* col_idx, uint64_t n, uint64_t m, gb_bfs** out) {

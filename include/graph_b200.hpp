@@ -81,6 +81,7 @@ struct GpuBfsOptions {
     uint64_t spinLimit = 0;              // grid-barrier wait bound in polls (0 = default)
     uint32_t gridBlocks = 0;             // blocks in the persistent grid (0 = every resident block)
     float selMargin = 0.5f;              // learned selector's direction margin (log2 of a time ratio)
+    uint32_t inFlight = 1;               // runMany: traversals run at once (1..4), each on a share of the SMs
 
     gb_bfs_options c() const {
         gb_bfs_options o;
@@ -98,6 +99,7 @@ struct GpuBfsOptions {
         o.spin_limit = spinLimit;
         o.grid_blocks = gridBlocks;
         o.sel_margin = selMargin;
+        o.in_flight = inFlight;
         return o;
     }
     static GpuBfsOptions fromC(const gb_bfs_options& o) {
@@ -115,6 +117,7 @@ struct GpuBfsOptions {
         r.spinLimit = o.spin_limit;
         r.gridBlocks = o.grid_blocks;
         r.selMargin = o.sel_margin;
+        r.inFlight = o.in_flight;
         return r;
     }
 };

@@ -121,3 +121,46 @@ def _device_dist(gb, bfs, n):
     err, = rt.cudaMemcpy(host.ctypes.data, ptr, 4 * n, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
     assert err == rt.cudaError_t.cudaSuccess
     return host
+
+
+@pytest.mark.parametrize("in_flight", [2, 3, 4])
+def test_run_many_several_in_flight(gb, oracle, in_flight):
+    """in_flight traversals at once, each on its own stream, state slot and
+    share of the SMs: every source's depths, in every packed width and in the
+    whole-buffer fallback, into separate rows, into one reused buffer (the last
+    source's), and kept on the device -- equal to the oracle's serial BFS, with
+    both selectors; more sources than depth buffers, so buffers are reused
+    across streams."""
+    g, first_path = _rmat_plus_path(gb, 2000)
+    og = _og(oracle, g)
+    power = [int(s) for s in gb.pick_sources(g, 14, 3) if s < first_path]
+    srcs = np.array(power[:4] + [first_path + 1000] + power[4:9] + [g.n - 1] + power[9:12], np.uint32)
+    want = [oracle.bfs_serial(og, int(s)) for s in srcs]
+    bfs = gb.GpuBfs(g).hub_first()
+    sels = [("rule", None)]
+    params = gb.default_selector_params("single")
+    if params is not None:
+        bfs.set_selector(params)
+        sels.append(("learned", params))
+    for sel, _ in sels:
+        o = gb.BfsOptions(selector=sel, in_flight=in_flight)
+        out, ms, lv = bfs.run_many("gpu_do_persistent", srcs, opts=o)
+        for i in range(len(srcs)):
+            assert np.array_equal(out[i], want[i]), (sel, i)
+            assert lv[i] == int(want[i][want[i] != 0xFFFFFFFF].max()) + 1
+        assert (ms > 0).all()
+        one = np.empty(g.n, np.uint32)
+        bfs.run_many("gpu_do_persistent", srcs, out=one, stride=0, opts=o)
+        assert np.array_equal(one, want[-1])
+        _, _, lv2 = bfs.run_many("gpu_do_persistent", srcs, opts=o, device=True)
+        assert np.array_equal(lv2, lv)
+        assert np.array_equal(_device_dist(gb, bfs, g.n), want[-1])
+        # a one-at-a-time call afterwards sees the same results
+        assert np.array_equal(bfs.run("gpu_do_persistent", int(srcs[3]), opts=gb.BfsOptions(selector=sel)), want[3])
+
+
+def test_run_many_in_flight_limits(gb):
+    bfs = gb.GpuBfs(gb.gen.rmat(12, 16, False, 3))
+    with pytest.raises(gb.GraphError) as e:
+        bfs.run_many("gpu_do_persistent", [0], opts=gb.BfsOptions(in_flight=5))
+    assert e.value.status == 1 and "in_flight" in str(e.value)
