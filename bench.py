@@ -889,7 +889,7 @@ def headline_workload(args, world, rank, local):
     # resident blocks, its own stream and state): the fastest K over this
     # rank's sources, by device time (untimed)
     flight_ms = {}
-    for k in (1, 2, 3, 4):
+    for k in ((args.in_flight,) if args.in_flight else (1, 2, 3, 4)):
         ok = G.BfsOptions(selector=opts.selector, block=opts.block, grid_blocks=0 if k > 1 else opts.grid_blocks,
                           hub_min=opts.hub_min, in_flight=k)
         bfs.run_many("gpu_do_persistent", srcs, opts=ok, device=True)
@@ -903,7 +903,7 @@ def headline_workload(args, world, rank, local):
             t_.append(ev0.elapsed_time(ev1))
         flight_ms[k] = (min(t_), ok)
     keys = sorted(flight_ms)
-    if world > 1:  # every rank runs the same number in flight
+    if world > 1 and not args.in_flight:  # every rank runs the same number in flight
         import torch.distributed as dist
         votes = torch.tensor([flight_ms[k][0] for k in keys], dtype=torch.float64, device="cuda")
         dist.all_reduce(votes, op=dist.ReduceOp.SUM)
@@ -1062,7 +1062,9 @@ def headline_workload(args, world, rank, local):
                     "speedup_learned_vs_rule": rule_ms / learned_ms,
                     "judge_ms_16_sources": {k: round(v[0], 4) for k, v in cands.items()},
                     "speedup_vs_plain_gpu_do": plain_ms / (total_ms / args.steps),
-                    "hmean_gteps_per_source": hmean},
+                    "hmean_gteps_per_source_launch": hmean,
+                    "hmean_note": "harmonic mean of per-source GTEPS from each launch's device time "
+                                  "(src/bench/main.cpp:366-370); launches overlap when in_flight > 1"},
     }
     if bad is not None:
         line["validation_failure"] = bad
@@ -1085,6 +1087,8 @@ def main():
     ap.add_argument("--fixed-opts", default="",
                     help="BLOCK,GRID,HUB: run the persistent / batched kernels with this launch shape and hub cut "
                          "instead of autotuning (profiling runs)")
+    ap.add_argument("--in-flight", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                    help="traversals at once in gb_bfs_run_many (0: measure 1-4 and keep the fastest)")
     ap.add_argument("--selector", default="rule", choices=["rule", "learned"],
                     help="with --fixed-opts: the per-level selector")
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (smaller: profiling cases)")
