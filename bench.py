@@ -889,7 +889,7 @@ def headline_workload(args, world, rank, local):
     # resident blocks, its own stream and state): the fastest K over this
     # rank's sources, by device time (untimed)
     flight_ms = {}
-    for k in ((args.in_flight,) if args.in_flight else (1, 2, 3, 4)):
+    for k in ((args.in_flight,) if args.in_flight else (1, 2, 3, 4, 6, 8)):
         ok = G.BfsOptions(selector=opts.selector, block=opts.block, grid_blocks=0 if k > 1 else opts.grid_blocks,
                           hub_min=opts.hub_min, in_flight=k)
         bfs.run_many("gpu_do_persistent", srcs, opts=ok, device=True)
@@ -1087,8 +1087,8 @@ def main():
     ap.add_argument("--fixed-opts", default="",
                     help="BLOCK,GRID,HUB: run the persistent / batched kernels with this launch shape and hub cut "
                          "instead of autotuning (profiling runs)")
-    ap.add_argument("--in-flight", type=int, default=0, choices=[0, 1, 2, 3, 4],
-                    help="traversals at once in gb_bfs_run_many (0: measure 1-4 and keep the fastest)")
+    ap.add_argument("--in-flight", type=int, default=0, choices=range(9),
+                    help="traversals at once in gb_bfs_run_many (0: measure 1, 2, 3, 4, 6, 8 and keep the fastest)")
     ap.add_argument("--selector", default="rule", choices=["rule", "learned"],
                     help="with --fixed-opts: the per-level selector")
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (smaller: profiling cases)")
