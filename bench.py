@@ -876,41 +876,44 @@ def headline_workload(args, world, rank, local):
             bfs.run("gpu_do_persistent", int(s_), opts=o)
             t_ += bfs.lastGpuMs()
         cands[name] = (t_, o)
-    if world > 1 and not args.fixed_opts:  # every rank must run the same selector and options
+    if world > 1 and not args.fixed_opts:  # every rank must run the same options
         import torch.distributed as dist
         votes = torch.tensor([cands[k][0] for k in sorted(cands)], dtype=torch.float64, device="cuda")
         dist.all_reduce(votes, op=dist.ReduceOp.SUM)
         selector = sorted(cands)[int(torch.argmin(votes))]
     else:
         selector = min(cands, key=lambda k: cands[k][0])
-    opts = cands[selector][1]
+    opts = cands[selector][1]  # the one-at-a-time judge; the in-flight choice below decides
     stream = torch.cuda.ExternalStream(G.lib().gb_bfs_stream(bfs._h))
     # traversals in flight in one gb_bfs_run_many call (each on 1/K of the
-    # resident blocks, its own stream and state): the fastest K over this
-    # rank's sources, by device time (untimed)
+    # resident blocks, its own stream and state): the selector and K of the
+    # fastest run_many over this rank's sources, by device time (untimed) --
+    # the configuration the timed steps run
     flight_ms = {}
-    for k in ((args.in_flight,) if args.in_flight else (1, 2, 3, 4, 6, 8)):
-        ok = G.BfsOptions(selector=opts.selector, block=opts.block, grid_blocks=0 if k > 1 else opts.grid_blocks,
-                          hub_min=opts.hub_min, in_flight=k)
-        bfs.run_many("gpu_do_persistent", srcs, opts=ok, device=True)
-        t_ = []
-        for _ in range(2):
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record(stream)
+    for name, (_, o_) in cands.items():
+        for k in ((args.in_flight,) if args.in_flight else (1, 2, 3, 4, 8, 12, 16)):
+            ok = G.BfsOptions(selector=o_.selector, block=o_.block, grid_blocks=0 if k > 1 else o_.grid_blocks,
+                              hub_min=o_.hub_min, in_flight=k)
             bfs.run_many("gpu_do_persistent", srcs, opts=ok, device=True)
-            ev1.record(stream)
-            ev1.synchronize()
-            t_.append(ev0.elapsed_time(ev1))
-        flight_ms[k] = (min(t_), ok)
+            t_ = []
+            for _ in range(3):
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+                bfs.run_many("gpu_do_persistent", srcs, opts=ok, device=True)
+                ev1.record(stream)
+                ev1.synchronize()
+                t_.append(ev0.elapsed_time(ev1))
+            flight_ms[(name, k)] = (min(t_), ok)
     keys = sorted(flight_ms)
-    if world > 1 and not args.in_flight:  # every rank runs the same number in flight
+    if world > 1:  # every rank runs the same selector and number in flight
         import torch.distributed as dist
         votes = torch.tensor([flight_ms[k][0] for k in keys], dtype=torch.float64, device="cuda")
         dist.all_reduce(votes, op=dist.ReduceOp.SUM)
-        in_flight = keys[int(torch.argmin(votes))]
+        best = keys[int(torch.argmin(votes))]
     else:
-        in_flight = min(keys, key=lambda k: flight_ms[k][0])
-    opts = flight_ms[in_flight][1]
+        best = min(keys, key=lambda k: flight_ms[k][0])
+    selector, in_flight = best
+    opts = flight_ms[best][1]
 
     max_levels = 0  # sets the packed depth width on the PCIe wire
     for s in srcs:
@@ -1029,7 +1032,7 @@ def headline_workload(args, world, rank, local):
         "method": {"selector": selector, "adjacency": args.adjacency,
                    "tuned": {"block": opts.block, "grid_blocks": opts.grid_blocks, "hub_min": opts.hub_min,
                              "in_flight": opts.in_flight},
-                   "in_flight_step_ms": {str(k): round(v[0], 3) for k, v in flight_ms.items()},
+                   "step_ms_by_selector_in_flight": {f"{k[0]}/{k[1]}": round(v[0], 3) for k, v in flight_ms.items()},
                    "call": "gb_bfs_run_many, one persistent launch per source; in_flight of them at once, "
                            "each on 1/in_flight of the resident blocks"},
         "work": {"edges_per_step": edges_all, "edges_per_step_rank0": edges_per_rank_step,
@@ -1060,6 +1063,9 @@ def headline_workload(args, world, rank, local):
                                                "hub_min": rule_opts.hub_min} if rule_opts is not None else None),
                     "persistent_learned_gteps": edges_per_rank_step / (learned_ms * 1e-3) / 1e9,
                     "speedup_learned_vs_rule": rule_ms / learned_ms,
+                    "speedup_learned_vs_rule_at_in_flight": (
+                        flight_ms[("rule", in_flight)][0] / flight_ms[("learned", in_flight)][0]
+                        if ("rule", in_flight) in flight_ms and ("learned", in_flight) in flight_ms else None),
                     "judge_ms_16_sources": {k: round(v[0], 4) for k, v in cands.items()},
                     "speedup_vs_plain_gpu_do": plain_ms / (total_ms / args.steps),
                     "hmean_gteps_per_source_launch": hmean,
@@ -1087,8 +1093,9 @@ def main():
     ap.add_argument("--fixed-opts", default="",
                     help="BLOCK,GRID,HUB: run the persistent / batched kernels with this launch shape and hub cut "
                          "instead of autotuning (profiling runs)")
-    ap.add_argument("--in-flight", type=int, default=0, choices=range(9),
-                    help="traversals at once in gb_bfs_run_many (0: measure 1, 2, 3, 4, 6, 8 and keep the fastest)")
+    ap.add_argument("--in-flight", type=int, default=0, choices=range(17),
+                    help="traversals at once in gb_bfs_run_many (0: measure 1, 2, 3, 4, 8, 12, 16 and keep the "
+                         "fastest)")
     ap.add_argument("--selector", default="rule", choices=["rule", "learned"],
                     help="with --fixed-opts: the per-level selector")
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (smaller: profiling cases)")

@@ -42,7 +42,7 @@ int packFormat(uint64_t count, uint32_t levels);
 uint64_t packedBytes(int fmt, uint64_t count);
 void enqueuePack(int fmt, const uint32_t* d, uint64_t count, uint8_t* dev, unsigned* overflow, cudaStream_t st);
 void widenPacked(int fmt, const uint8_t* in, uint64_t count, uint32_t* out);
-constexpr int kMaxInFlight = 8;              // traversals at once in gb_bfs::runPersistentMany
+constexpr int kMaxInFlight = 16;              // traversals at once in gb_bfs::runPersistentMany
 constexpr int kManySlots = kMaxInFlight + 2;  // depth buffers it rotates (in flight + 2)
 }  // namespace gb
 

@@ -203,7 +203,7 @@ typedef struct {
                             the time ratio); its top-down strategy choice is free.  0 = pure
                             argmin.  A direction change costs work the per-level predictions do
                             not see (a bottom-up to top-down switch rebuilds the queue). */
-    uint32_t in_flight;  /* gb_bfs_run_many, persistent variant: traversals run at once (1..8; 0 = 1),
+    uint32_t in_flight;  /* gb_bfs_run_many, persistent variant: traversals run at once (1..16; 0 = 1),
                             each a cooperative grid of grid_blocks (0 = every resident block /
                             in_flight) with its own state and stream.  A traversal's levels are
                             bound by dependent loads and the grid barrier, so two or more of

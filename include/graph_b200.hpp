@@ -81,7 +81,7 @@ struct GpuBfsOptions {
     uint64_t spinLimit = 0;              // grid-barrier wait bound in polls (0 = default)
     uint32_t gridBlocks = 0;             // blocks in the persistent grid (0 = every resident block)
     float selMargin = 0.5f;              // learned selector's direction margin (log2 of a time ratio)
-    uint32_t inFlight = 1;               // runMany: traversals run at once (1..8), each on a share of the SMs
+    uint32_t inFlight = 1;               // runMany: traversals run at once (1..16), each on a share of the SMs
 
     gb_bfs_options c() const {
         gb_bfs_options o;

@@ -123,7 +123,7 @@ def _device_dist(gb, bfs, n):
     return host
 
 
-@pytest.mark.parametrize("in_flight", [2, 3, 4, 8])
+@pytest.mark.parametrize("in_flight", [2, 3, 4, 8, 16])
 def test_run_many_several_in_flight(gb, oracle, in_flight):
     """in_flight traversals at once, each on its own stream, state slot and
     share of the SMs: every source's depths, in every packed width and in the
@@ -162,5 +162,5 @@ def test_run_many_several_in_flight(gb, oracle, in_flight):
 def test_run_many_in_flight_limits(gb):
     bfs = gb.GpuBfs(gb.gen.rmat(12, 16, False, 3))
     with pytest.raises(gb.GraphError) as e:
-        bfs.run_many("gpu_do_persistent", [0], opts=gb.BfsOptions(in_flight=9))
+        bfs.run_many("gpu_do_persistent", [0], opts=gb.BfsOptions(in_flight=17))
     assert e.value.status == 1 and "in_flight" in str(e.value)
