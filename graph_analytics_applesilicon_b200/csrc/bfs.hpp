@@ -2,6 +2,7 @@
 // src/metal/bfs_gpu.hpp:35-105).
 #pragma once
 
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
@@ -85,7 +86,7 @@ struct gb_bfs {
         gb::DevBuf<double> state;
     };
     PSlot pSlot[gb::kMaxInFlight - 1];
-    gb::Stream pStream[gb::kMaxInFlight - 1];
+    std::unique_ptr<gb::Stream> pStream[gb::kMaxInFlight - 1];  // created on first use
 
     // batched (64 sources)
     gb::DevBuf<unsigned long long> bSeen, bFront[2], bNext;

@@ -940,7 +940,10 @@ void gb_bfs::runPersistentMany(const uint32_t* src, uint32_t count, uint32_t* ou
     for (uint32_t b = 1; b < B; ++b) bufs[b] = mDist[b - 1].get();
     cudaStream_t streams[kMaxInFlight];
     streams[0] = stream.s;
-    for (uint32_t k = 1; k < K; ++k) streams[k] = pStream[k - 1].s;
+    for (uint32_t k = 1; k < K; ++k) {
+        if (!pStream[k - 1]) pStream[k - 1] = std::make_unique<gb::Stream>();
+        streams[k] = pStream[k - 1]->s;
+    }
     cudaEvent_t startEv = mSlotEv[3 * kManySlots];
     std::vector<int> fmt(count, -1);
     // packed width: from the most levels among this call's finished sources,
