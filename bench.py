@@ -1050,7 +1050,8 @@ def headline_workload(args, world, rank, local):
                      "kernel": kernel, "bytes_per_launch": bytes_per_trav,
                      "mean_launch_ms": mean_launch, "launches_at_once": opts.in_flight,
                      "achieved_basis": "bytes of the step's launches / device step time",
-                     "dram_achieved": (traffic / (mean_launch * 1e-3) / 1e9) if traffic else None},
+                     "dram_achieved": (traffic * len(srcs) / (statistics.mean(step_ms) * 1e-3) / 1e9)
+                     if traffic else None},
         "cpu_baseline": cpu if world == 1 else None,
         "clocks": clocks.summary(),
         "validated": valid,
