@@ -579,23 +579,33 @@ __global__ void prPushFinalizeKernel(PrArgs a) {
 // ---------------------------------------------------------------- blocked pull
 // Rows in row blocks whose sums live in shared memory, columns in parts of
 // kBlkPart vertices whose contributions are staged in shared memory, so no
-// gather reaches L2: an edge costs one 4-byte streaming read from DRAM, one
-// shared-memory gather and one shared-memory float atomic add.  One CUDA
-// block of kBlkThreads per row block (one per SM at the graph sizes this form
-// is for), looping over the column parts starting at a part that depends on
-// the row block (the SMs then stage different contributions at once).  Part
-// j + 1's contributions arrive in the other half of a two-part ring by one
-// TMA bulk copy (cp.async.bulk, completion counted on that half's mbarrier)
-// while part j's edges are summed, and every thread holds the first
-// kBlkEdgeRegs 16-byte words of its share of part j + 1's edges in registers
-// by then; one block barrier per part frees the ring half for the next copy.
-// Every thread takes an equal share of each tile's edges (no row ownership,
-// so no warp waits for another's heavier rows).  Rows with kBlkHub or more
-// in-edges are summed afterwards by one block each with Kahan-compensated
-// per-thread sums combined as float-float; the other rows' sums are plain
-// FP32 (fewer than kBlkHub terms).  Every mbarrier wait is bounded: on a
-// timeout the block records the error in the control block, waits (bounded)
-// for its copy in flight and leaves without storing.
+// gather reaches L2: an edge costs 4 bytes of a streamed tile, one shared-
+// memory gather and one shared-memory float atomic add.  One CUDA block of
+// kBlkThreads per row block (one per SM at the graph sizes this form is for),
+// warp-specialized:
+//   warp 0, one thread: the producer.  It walks the block's non-empty tiles
+//     (row block k, part p), parts in an order rotated by k so the SMs stage
+//     different contributions at once, and issues TMA bulk copies
+//     (cp.async.bulk) of part p's contributions into a ring of kBlkCStages
+//     stages and of the tile's packed edge words, in chunks of at most
+//     kBlkChunk words, into a ring of kBlkEStages stages.  Each copy completes
+//     on its stage's `full` mbarrier; a stage is refilled only after every
+//     consumer warp has arrived on its `empty` mbarrier.
+//   warps 1..kBlkConsumerWarps: the consumers.  For every chunk each thread
+//     takes one 16-byte word (four edges) from the edge ring and adds the
+//     staged contributions into the row sums.  Warps wait only on the stages
+//     they read, so they drift across parts and row blocks; no block barrier
+//     runs per part.  A named barrier among the consumers separates row
+//     blocks (sums stored, then zeroed for the next block).
+// The producer runs up to kBlkCStages parts and kBlkEStages chunks ahead,
+// across row-block boundaries.  Rows with kBlkHub or more in-edges are summed
+// afterwards by one block each with Kahan-compensated per-thread sums
+// combined as float-float; the other rows' sums are plain FP32 (fewer than
+// kBlkHub terms).  Every mbarrier wait is bounded: a thread whose wait gives
+// up raises the block's failure flag and stops issuing or consuming; the
+// others then time out on the stages it no longer fills or frees, the
+// consumers agree at their named barrier, the producer waits (bounded) for
+// the copies it has in flight, and the block records the error and leaves.
 struct BlkArgs {
     const uint4* edges;     // tiles of packed (row in block << 16 | column in part) words, 0xFFFFFFFF padding
     const uint32_t* off;    // 16-byte-word offset of tile (k, p) at k * nParts + p, then the end
@@ -621,12 +631,31 @@ __device__ __forceinline__ bool blkWait(unsigned long long* mbar, uint32_t parit
     return false;
 }
 
-__device__ __forceinline__ uint4 ldStream16(const uint4* p) {
-    uint4 v;
-    asm("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
-        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-        : "l"(p));
-    return v;
+__device__ __forceinline__ void blkArrive(unsigned long long* mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(mbar)) : "memory");
+}
+
+// One bulk copy of `bytes` (a multiple of 16, both addresses 16-byte
+// aligned) from global memory into shared memory, completing on `mbar`.
+__device__ __forceinline__ void blkCopy(void* dst, const void* src, uint32_t bytes, unsigned long long* mbar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(mbar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smemAddr(dst)),
+                 "l"(src), "r"(bytes), "r"(smemAddr(mbar))
+                 : "memory");
+}
+
+// Named barrier 1 among the consumer threads; returns whether any of them
+// passed `pred`.
+__device__ __forceinline__ bool consumersOr(bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbarrier.cta.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "n"(kBlkConsumerWarps * 32)
+        : "memory");
+    return r != 0;
 }
 
 // The four edges of one 16-byte word into the row sums.
@@ -638,105 +667,131 @@ __device__ __forceinline__ void blkAdd(float* sums, const float* part, uint4 w) 
 }
 
 __global__ void __launch_bounds__(kBlkThreads, 1) prBlockedKernel(PrArgs a, BlkArgs b) {
-    // [0, 2 kBlkPart): the contribution ring; then the row block's sums
+    // [contribution ring][edge ring][row sums]
     extern __shared__ __align__(128) float blkSmem[];
-    __shared__ __align__(8) unsigned long long full[2];
+    float* cring = blkSmem;
+    uint4* ering = reinterpret_cast<uint4*>(blkSmem + kBlkCStages * kBlkPart);
+    float* sums = reinterpret_cast<float*>(ering + kBlkEStages * kBlkChunk);
+    __shared__ __align__(8) unsigned long long cFull[kBlkCStages], cEmpty[kBlkCStages];
+    __shared__ __align__(8) unsigned long long eFull[kBlkEStages], eEmpty[kBlkEStages];
+    __shared__ int sFailed;
     const GbPrControl* c = a.ctl;
     if (ldvi(&c->stopped)) return;
     const int cur = c->cur;
     const bool withDelta = c->withDelta;
     const float dang = c->dangHi + c->dangLo;
     const float* contrib = a.contrib[cur];
-    float* sums = blkSmem + 2 * kBlkPart;
-    const unsigned tid = threadIdx.x;
+    const unsigned tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) {
-        for (int h = 0; h < 2; ++h)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(&full[h])) : "memory");
+        for (int i = 0; i < kBlkCStages; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(&cFull[i])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(&cEmpty[i])),
+                         "r"(kBlkConsumerWarps)
+                         : "memory");
+        }
+        for (int i = 0; i < kBlkEStages; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(&eFull[i])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(&eEmpty[i])),
+                         "r"(kBlkConsumerWarps)
+                         : "memory");
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        sFailed = 0;
     }
     __syncthreads();
-    IterAcc acc;
-    uint32_t t = 0;        // parts staged so far: part t uses ring half t & 1, fill number t >> 1
-    bool failed = false;
-    for (uint32_t k = blockIdx.x; k < b.nRowBlocks && !failed; k += gridDim.x) {
-        const uint32_t r0 = k * b.rowsPer, rows = min(a.n - r0, b.rowsPer);
-        for (uint32_t i = tid; i < rows; i += kBlkThreads) sums[i] = 0.0f;
+    auto tileOf = [&](uint32_t k, uint32_t j, uint32_t& w0, uint32_t& w1) {
         const uint32_t rot = (uint32_t)((uint64_t)k * b.nParts / b.nRowBlocks);
-        auto partAt = [&](uint32_t j) { return j + rot < b.nParts ? j + rot : j + rot - b.nParts; };
-        // part p's contributions into ring half h: one bulk copy of whole
-        // 16-byte groups (the contribution arrays carry 4 floats of slack past n)
-        auto stage = [&](uint32_t p, uint32_t h) {
-            if (tid != 0) return;
-            const uint32_t first = p * kBlkPart;
-            const uint32_t bytes = ((min(kBlkPart, a.n - first) * 4u) + 15u) & ~15u;
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(&full[h])),
-                         "r"(bytes)
-                         : "memory");
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                    smemAddr(blkSmem + h * kBlkPart)),
-                "l"(contrib + first), "r"(bytes), "r"(smemAddr(&full[h]))
-                : "memory");
-        };
-        // this thread's first kBlkEdgeRegs words of tile (k, p)
-        auto loadEdges = [&](uint32_t p, uint4 (&e)[kBlkEdgeRegs], uint32_t& w0, uint32_t& w1) {
-            const uint64_t g = (uint64_t)k * b.nParts + p;
-            w0 = b.off[g];
-            w1 = b.off[g + 1];
-#pragma unroll
-            for (int q = 0; q < kBlkEdgeRegs; ++q) {
-                const uint32_t i = w0 + tid + q * kBlkThreads;
-                e[q] = i < w1 ? ldStream16(b.edges + i) : make_uint4(~0u, ~0u, ~0u, ~0u);
-            }
-        };
-        uint4 e[kBlkEdgeRegs];
-        uint32_t w0, w1;
-        // the block barrier at the end of the previous row block (or the
-        // mbarrier set-up) has freed both ring halves
-        stage(partAt(0), t & 1u);
-        loadEdges(partAt(0), e, w0, w1);
-        for (uint32_t j = 0; j < b.nParts; ++j, ++t) {
-            const bool ok = blkWait(&full[t & 1u], (t >> 1) & 1u, b.spinLimit);
-            // part j is staged; every thread is done with part j - 1, whose
-            // ring half the next copy overwrites; the block agrees on a timeout
-            if (__syncthreads_or(!ok)) {
-                failed = true;
-                break;
-            }
-            uint4 en[kBlkEdgeRegs];
-            uint32_t n0 = 0, n1 = 0;
-            if (j + 1 < b.nParts) {
-                stage(partAt(j + 1), (t + 1) & 1u);
-                loadEdges(partAt(j + 1), en, n0, n1);
-            }
-            const float* part = blkSmem + (t & 1u) * kBlkPart;
-#pragma unroll
-            for (int q = 0; q < kBlkEdgeRegs; ++q) blkAdd(sums, part, e[q]);
-            for (uint32_t i = w0 + tid + kBlkEdgeRegs * kBlkThreads; i < w1; i += kBlkThreads)
-                blkAdd(sums, part, ldStream16(b.edges + i));
-#pragma unroll
-            for (int q = 0; q < kBlkEdgeRegs; ++q) e[q] = en[q];
-            w0 = n0;
-            w1 = n1;
-        }
-        if (failed) break;
-        __syncthreads();
-        for (uint32_t i = tid; i < rows; i += kBlkThreads) {
-            const uint32_t v = r0 + i;
-            if (a.rp[v + 1] - a.rp[v] >= kBlkHub) continue;
-            storeJacobi(a, cur, withDelta, v, prValue(a, sums[i], dang), acc);
-        }
-        __syncthreads();  // the next row block zeroes the sums and refills the ring
-    }
-    if (failed) {
-        // the block stopped at part t before issuing the next copy, so part
-        // t's own copy is the only one that may still be landing: let it
-        // arrive (bounded) before the block's shared memory is released
+        const uint32_t p = j + rot < b.nParts ? j + rot : j + rot - b.nParts;
+        const uint64_t g = (uint64_t)k * b.nParts + p;
+        w0 = b.off[g];
+        w1 = b.off[g + 1];
+        return p;
+    };
+    IterAcc acc;
+    if (warp == 0) {
         if (tid == 0) {
-            atomicOr(&a.ctl->error, 1);
-            blkWait(&full[t & 1u], (t >> 1) & 1u, b.spinLimit);
+            // producer: parts staged (ci) and chunks issued (ei) so far
+            uint32_t ci = 0, ei = 0;
+            bool ok = true;
+            for (uint32_t k = blockIdx.x; k < b.nRowBlocks && ok; k += gridDim.x) {
+                for (uint32_t j = 0; j < b.nParts && ok; ++j) {
+                    uint32_t w0, w1;
+                    const uint32_t p = tileOf(k, j, w0, w1);
+                    if (w0 == w1) continue;
+                    const uint32_t cs = ci % kBlkCStages;
+                    if (ci >= kBlkCStages) ok = blkWait(&cEmpty[cs], (ci / kBlkCStages - 1) & 1u, b.spinLimit);
+                    if (!ok) break;
+                    // whole 16-byte groups: the contribution arrays carry 4 floats of slack past n
+                    const uint32_t first = p * kBlkPart;
+                    const uint32_t bytes = ((min(kBlkPart, (uint32_t)a.n - first) * 4u) + 15u) & ~15u;
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    blkCopy(cring + cs * kBlkPart, contrib + first, bytes, &cFull[cs]);
+                    ++ci;
+                    for (uint32_t w = w0; w < w1; w += kBlkChunk) {
+                        const uint32_t es = ei % kBlkEStages;
+                        if (ei >= kBlkEStages) ok = blkWait(&eEmpty[es], (ei / kBlkEStages - 1) & 1u, b.spinLimit);
+                        if (!ok) break;
+                        const uint32_t words = min(kBlkChunk, w1 - w);
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        blkCopy(ering + es * kBlkChunk, b.edges + w, words * 16u, &eFull[es]);
+                        ++ei;
+                    }
+                }
+            }
+            if (!ok) atomicOr(&sFailed, 1);
+            // every copy issued must land before the block's shared memory is
+            // released: wait for the last fill of each stage (bounded)
+            for (uint32_t x = ci > kBlkCStages ? ci - kBlkCStages : 0; x < ci; ++x)
+                if (!blkWait(&cFull[x % kBlkCStages], (x / kBlkCStages) & 1u, b.spinLimit)) atomicOr(&sFailed, 1);
+            for (uint32_t x = ei > kBlkEStages ? ei - kBlkEStages : 0; x < ei; ++x)
+                if (!blkWait(&eFull[x % kBlkEStages], (x / kBlkEStages) & 1u, b.spinLimit)) atomicOr(&sFailed, 1);
         }
+        __syncwarp();  // lanes 1-31 wait for the producer thread
+    } else {
+        // consumers: thread ct of kBlkConsumerWarps * 32
+        const unsigned ct = tid - 32, lane = tid & 31;
+        constexpr unsigned kCons = kBlkConsumerWarps * 32;
+        uint32_t ci = 0, ei = 0;
+        bool ok = true;
+        for (uint32_t k = blockIdx.x; k < b.nRowBlocks; k += gridDim.x) {
+            const uint32_t r0 = k * b.rowsPer, rows = min((uint32_t)a.n - r0, b.rowsPer);
+            for (uint32_t i = ct; i < rows; i += kCons) sums[i] = 0.0f;
+            if (consumersOr(!ok)) break;  // sums zeroed (and the previous block's stored)
+            for (uint32_t j = 0; j < b.nParts && ok; ++j) {
+                uint32_t w0, w1;
+                tileOf(k, j, w0, w1);
+                if (w0 == w1) continue;
+                const uint32_t cs = ci % kBlkCStages;
+                ok = __all_sync(kFull, blkWait(&cFull[cs], (ci / kBlkCStages) & 1u, b.spinLimit));
+                if (!ok) break;
+                const float* part = cring + cs * kBlkPart;
+                for (uint32_t w = w0; w < w1; w += kBlkChunk) {
+                    const uint32_t es = ei % kBlkEStages;
+                    ok = __all_sync(kFull, blkWait(&eFull[es], (ei / kBlkEStages) & 1u, b.spinLimit));
+                    if (!ok) break;
+                    const uint32_t words = min(kBlkChunk, w1 - w);
+                    for (uint32_t q = ct; q < words; q += kCons) blkAdd(sums, part, ering[es * kBlkChunk + q]);
+                    __syncwarp();
+                    if (lane == 0) blkArrive(&eEmpty[es]);
+                    ++ei;
+                }
+                if (!ok) break;
+                __syncwarp();
+                if (lane == 0) blkArrive(&cEmpty[cs]);
+                ++ci;
+            }
+            if (consumersOr(!ok)) break;  // every edge of row block k is in the sums
+            for (uint32_t i = ct; i < rows; i += kCons) {
+                const uint32_t v = r0 + i;
+                if (a.rp[v + 1] - a.rp[v] >= kBlkHub) continue;
+                storeJacobi(a, cur, withDelta, v, prValue(a, sums[i], dang), acc);
+            }
+        }
+        if (!ok && lane == 0) atomicOr(&sFailed, 1);
+    }
+    __syncthreads();
+    if (sFailed) {
+        if (tid == 0) atomicOr(&a.ctl->error, 1);
         return;
     }
     // rows with kBlkHub or more in-edges: one block each
@@ -874,7 +929,8 @@ uint32_t residentGrid(K kernel, uint64_t work, uint32_t threads) {
 // the opt-in limit is raised once per process.
 static size_t blkSmemBytes() {
     static const size_t bytes = [] {
-        const size_t b = ((size_t)2 * kBlkPart + kBlkRowCap) * sizeof(float);
+        const size_t b = ((size_t)kBlkCStages * kBlkPart + kBlkRowCap) * sizeof(float) +
+                         (size_t)kBlkEStages * kBlkChunk * sizeof(uint4);
         GB_CUDA(cudaFuncSetAttribute(prBlockedKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b));
         return b;
     }();

@@ -38,16 +38,20 @@ struct GbPrControl {
 
 // Blocked pull (GB_PR_PULL_BLOCKED): rows in blocks of at most kBlkRowCap
 // (their sums in shared memory, one CUDA block per row block), columns in
-// parts of kBlkPart vertices (their contributions staged in shared memory,
-// two parts at a time); tile (row block, part) holds that block's edges from
-// that part as packed 32-bit words.  Each thread prefetches kBlkEdgeRegs
-// 16-byte words of the next tile.  Rows with kBlkHub or more in-edges are
-// summed apart.
-constexpr uint32_t kBlkPart = 16384;
+// parts of kBlkPart vertices (their contributions staged in shared memory by
+// TMA, kBlkCStages parts at a time); tile (row block, part) holds that block's
+// edges from that part as packed 32-bit words, staged by TMA in chunks of at
+// most kBlkChunk 16-byte words, kBlkEStages chunks at a time.  One producer
+// warp issues the copies; kBlkConsumerWarps warps add the edges.  Rows with
+// kBlkHub or more in-edges are summed apart.
+constexpr uint32_t kBlkPart = 8192;
 constexpr uint32_t kBlkRowCap = 21504;
-constexpr int kBlkEdgeRegs = 3;
-constexpr uint32_t kBlkHub = 4096;  // rows with this many in-edges are summed apart, one block each
+constexpr int kBlkCStages = 2;
+constexpr int kBlkEStages = 4;
 constexpr int kBlkThreads = 1024;
+constexpr int kBlkConsumerWarps = kBlkThreads / 32 - 1;
+constexpr uint32_t kBlkChunk = kBlkConsumerWarps * 32;  // one 16-byte word per consumer thread
+constexpr uint32_t kBlkHub = 4096;  // rows with this many in-edges are summed apart, one block each
 
 struct gb_pr {
     uint64_t n = 0, mOut = 0, mIn = 0;
