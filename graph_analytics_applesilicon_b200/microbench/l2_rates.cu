@@ -1,9 +1,8 @@
-// l2_rates.cu -- the L2 rates the PageRank kernels are measured against:
+// l2_rates.cu -- the L2 staging rates the blocked PageRank pull is measured against:
 //  * TMA bulk copies (cp.async.bulk) of S bytes from an L2-resident 12 MiB array
 //    into a ring of D shared-memory stages, one producer thread per block;
-//  * 16-byte loads by every thread (ld.global.cg) of the same array;
-//  * random 4-byte gathers from it through L2 (ld.global.cg) and through the
-//    read-only path (ld.global.nc), over the whole array and over 64-256 KB windows.
+//  * 16-byte loads by every thread (ld.global.cg) of the same array.
+// (Gather rates are measured on a graph's own in-lists by gather_bound.py.)
 // Every wait is bounded (an error flag instead of a hang) and every index is
 // reduced into its array.  Build and run on one GPU:
 //   nvcc -gencode arch=compute_100a,code=sm_100a -O3 -o l2_rates \
@@ -74,19 +73,6 @@ __global__ void vecLoad(const uint4* src, size_t nchunks, uint32_t S, int K, flo
     }
     if (acc == 12345.f) sink[0] = acc;
 }
-__device__ __forceinline__ uint32_t hash32(uint32_t x) { x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16; return x; }
-__global__ void gather(const float* arr, uint32_t n, uint32_t win, int G, int cached, float* sink) {
-    float acc = 0;
-    uint32_t base = (uint32_t)(((uint64_t)blockIdx.x * 7919u * win) % (uint64_t)(n - win + 1));
-    uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int g = 0; g < G; g += 4) {
-        uint32_t i0 = hash32(h + g * 0x9E3779B9u) % win, i1 = hash32(h + g * 0x9E3779B9u + 1) % win;
-        uint32_t i2 = hash32(h + g * 0x9E3779B9u + 2) % win, i3 = hash32(h + g * 0x9E3779B9u + 3) % win;
-        if (cached) acc += __ldg(arr + base + i0) + __ldg(arr + base + i1) + __ldg(arr + base + i2) + __ldg(arr + base + i3);
-        else acc += __ldcg(arr + base + i0) + __ldcg(arr + base + i1) + __ldcg(arr + base + i2) + __ldcg(arr + base + i3);
-    }
-    if (acc == 12345.f) sink[0] = acc;
-}
 int main() {
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
@@ -113,14 +99,6 @@ int main() {
         CK(cudaEventRecord(e0)); vecLoad<<<sms * bps, 1024 / bps>>>((const uint4*)src, nchunks, S, K, sink); CK(cudaEventRecord(e1));
         CK(cudaEventSynchronize(e1)); float ms; CK(cudaEventElapsedTime(&ms, e0, e1));
         printf("LDG.128 S=%6u blocks/SM=%d: %.3f ms, %.2f TB/s\n", S, bps, ms, (double)K * S * sms * bps / ms / 1e9);
-    }
-    const uint32_t n = (uint32_t)(nbytes / 4);
-    for (uint32_t win : {n, 16384u, 32768u, 65536u}) for (int cached : {0, 1}) {
-        int G = 256, blocks = sms * 2, thr = 1024;
-        gather<<<blocks, thr>>>((const float*)src, n, win, G, cached, sink);
-        CK(cudaEventRecord(e0)); gather<<<blocks, thr>>>((const float*)src, n, win, G, cached, sink); CK(cudaEventRecord(e1));
-        CK(cudaEventSynchronize(e1)); float ms; CK(cudaEventElapsedTime(&ms, e0, e1));
-        printf("gather win=%8u %s: %.3f ms, %.1f G/s\n", win, cached ? "ldg" : "ldcg", ms, (double)blocks * thr * G / ms / 1e6);
     }
     int herr; CK(cudaMemcpy(&herr, err, 4, cudaMemcpyDeviceToHost)); printf("err %d\n", herr);
     return 0;
