@@ -27,6 +27,21 @@ namespace {
 constexpr unsigned long long kHubShift = 40;
 constexpr unsigned long long kHubMask = (1ull << kHubShift) - 1;
 constexpr uint32_t kTraceCap = 1u << 16;
+#ifndef GB_BATCH_BU_SERIAL
+#define GB_BATCH_BU_SERIAL 64
+#endif
+#ifndef GB_BATCH_BU_COOP
+#define GB_BATCH_BU_COOP 64
+#endif
+#ifndef GB_BATCH_BU_BLOCK
+#define GB_BATCH_BU_BLOCK 512
+#endif
+// bottom-up list scans: serial per thread for the first kBatchBuSerial entries,
+// then a rest of kBatchBuCoop entries or more by the warp, kBatchBuBlock or
+// more by the block
+constexpr uint32_t kBatchBuSerial = GB_BATCH_BU_SERIAL;
+constexpr uint32_t kBatchBuCoop = GB_BATCH_BU_COOP;
+constexpr uint32_t kBatchBuBlock = GB_BATCH_BU_BLOCK;
 
 struct BCounters {
     unsigned acnt;                 // next active queue entries
@@ -98,6 +113,10 @@ struct BSmem {
     int strat;
     uint32_t base;
     int ok;
+    uint32_t hmask[NT / 32];  // bottom-up: lanes whose list the whole block scans
+    unsigned bor[2];          // OR of the frontier masks found so far (lo, hi)
+    uint32_t hst, hd;
+    unsigned long long hneed;
 };
 
 // Grid barrier after which every thread of the block sees counters *c in
@@ -389,26 +408,111 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
             const unsigned long long* fc = a.fr[qc];
             for (uint64_t base = (uint64_t)blockIdx.x * NT; base < a.n; base += gthreads) {
                 const uint64_t v = base + tid;
-                unsigned long long b = 0, old = 0;
+                unsigned long long b = 0, old = 0, need = 0;
                 uint32_t st = 0, d = 0;
                 if (v < a.n) {
                     old = a.seen[v];
-                    const unsigned long long need = a.all & ~old;
+                    need = a.all & ~old;
                     st = a.row_ptr[v];
                     d = a.row_ptr[v + 1] - st;
-                    if (need) {
-                        // OR the neighbours' frontier masks until every missing
-                        // source is covered; aligned groups of 4 entries are
-                        // loaded at once with their 4 masks.
-                        unsigned long long got = 0;
-                        uint32_t i = st;
-                        const uint32_t e = st + d;
-                        for (; i < e && (i & 3u) && (got & need) != need; ++i) got |= fc[a.col_idx[i]];
-                        for (; i + 4 <= e && (got & need) != need; i += 4) {
-                            const uint4 q = *reinterpret_cast<const uint4*>(a.col_idx + i);
-                            got |= fc[q.x] | fc[q.y] | fc[q.z] | fc[q.w];
+                }
+                // Each thread ORs its vertex's neighbours' frontier masks until
+                // every missing source is covered (most lists stop early), for
+                // at most kBatchBuSerial entries; aligned groups of 4 entries
+                // are loaded at once with their 4 masks.  What is left of a
+                // list then goes to the whole warp (kBatchBuCoop or more
+                // entries left: the warp takes such lists one after another,
+                // 128 entries per step) or to the whole block (kBatchBuBlock or
+                // more left, 4 NT entries per step); shorter rests finish
+                // serially.  One long list scanned by one thread would hold its
+                // warp, its block and the level.
+                unsigned long long got = 0;
+                uint32_t i = st;
+                const uint32_t e = st + d;
+                auto scanTo = [&](uint32_t lim) {
+                    for (; i < lim && (i & 3u) && (got & need) != need; ++i) got |= fc[a.col_idx[i]];
+                    for (; i + 4 <= lim && (got & need) != need; i += 4) {
+                        const uint4 q = *reinterpret_cast<const uint4*>(a.col_idx + i);
+                        got |= fc[q.x] | fc[q.y] | fc[q.z] | fc[q.w];
+                    }
+                    for (; i < lim && (got & need) != need; ++i) got |= fc[a.col_idx[i]];
+                };
+                if (need) scanTo(st + min(d, kBatchBuSerial));
+                const uint32_t rest = (need && (got & need) != need) ? e - i : 0u;
+                const bool huge = rest >= kBatchBuBlock;
+                const bool coop = !huge && rest >= kBatchBuCoop;
+                if (rest && !huge && !coop) scanTo(e);
+                const unsigned long long want = need & ~got;  // still missing after the serial part
+                for (unsigned hm = __ballot_sync(kFull, coop); hm; hm &= hm - 1) {
+                    const int l = __ffs(hm) - 1;
+                    const uint32_t hs = __shfl_sync(kFull, i, l), hd = __shfl_sync(kFull, e, l) - hs;
+                    const unsigned long long hn = __shfl_sync(kFull, want, l);
+                    unsigned long long g2 = 0;
+                    uint32_t off = 0;
+                    while (off < hd) {
+                        unsigned long long g = 0;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const uint32_t j = off + laneId() + 32u * q;
+                            if (j < hd) g |= fc[a.col_idx[hs + j]];
                         }
-                        for (; i < e && (got & need) != need; ++i) got |= fc[a.col_idx[i]];
+                        g2 |= warpOr64(g);
+                        off += 128;
+                        if ((g2 & hn) == hn) break;
+                    }
+                    if (laneId() == (unsigned)l) {
+                        got |= g2;
+                        i += min(off, hd);
+                    }
+                }
+                {
+                    const unsigned hw = __ballot_sync(kFull, huge);
+                    if (laneId() == 0) sm.hmask[tid >> 5] = hw;
+                }
+                if (__syncthreads_or(huge)) {
+                    for (int w = 0; w < NT / 32; ++w) {
+                        for (unsigned hm = sm.hmask[w]; hm; hm &= hm - 1) {
+                            const unsigned owner = (unsigned)w * 32u + (unsigned)(__ffs(hm) - 1);
+                            if (tid == owner) {
+                                sm.hst = i;
+                                sm.hd = e - i;
+                                sm.hneed = want;
+                                sm.bor[0] = 0;
+                                sm.bor[1] = 0;
+                            }
+                            __syncthreads();
+                            const uint32_t hs = sm.hst, hd = sm.hd;
+                            const unsigned long long hn = sm.hneed;
+                            unsigned long long g2 = 0;
+                            uint32_t off = 0;
+                            while (off < hd) {
+                                unsigned long long g = 0;
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    const uint32_t j = off + tid + (uint32_t)NT * q;
+                                    if (j < hd) g |= fc[a.col_idx[hs + j]];
+                                }
+                                g = warpOr64(g);
+                                if (laneId() == 0 && g) {
+                                    atomicOr(&sm.bor[0], (unsigned)g);
+                                    atomicOr(&sm.bor[1], (unsigned)(g >> 32));
+                                }
+                                __syncthreads();
+                                g2 = ((unsigned long long)sm.bor[1] << 32) | sm.bor[0];
+                                off += 4u * NT;
+                                if ((g2 & hn) == hn) break;  // block-uniform: all read bor between barriers
+                                __syncthreads();
+                            }
+                            if (tid == owner) {
+                                got |= g2;
+                                i += min(off, hd);
+                            }
+                            __syncthreads();
+                        }
+                    }
+                }
+                if (v < a.n) {
+                    if (need) {
                         acc.exam += i - st;
                         b = got & need;
                     }

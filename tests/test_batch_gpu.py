@@ -74,3 +74,43 @@ def test_batch_learned_selector_exact(gb, oracle):
     for _ in range(3):
         bfs.set_selector(rng.normal(0, 1, gb.selector_param_count()).astype(np.float32), 1)
         check_batch(gb, oracle, g, bfs, srcs, gb.BfsOptions(selector="learned"))
+
+
+def test_batch_bottom_up_long_lists_exact(gb, oracle):
+    """Bottom-up levels hand what is left of a long list to the whole warp
+    (64 or more entries left after the thread's own first 64) or to the whole
+    block (512 or more).  Hubs of 100 to 6,000 neighbours in one component and
+    half of the sources in another component keep every hub's missing sources
+    missing, so its scan runs to the end of its list; lists that finish early
+    and short rests finishing serially are in the same warps.  Every source's
+    depths must equal the oracle's, forced bottom-up and under the rule, on
+    both adjacency orders."""
+    rng = np.random.default_rng(11)
+    n1 = 20000
+    eu, ev = [], []
+    for hub, deg in ((0, 6000), (1, 3000), (2, 700), (3, 513), (4, 200), (5, 100), (6, 65)):
+        nb = rng.choice(np.arange(7, n1), deg, replace=False)
+        eu.append(np.full(deg, hub)); ev.append(nb)
+    # a sparse random graph on the rest of component A, and a path joining the hubs
+    eu.append(rng.integers(7, n1, 3 * n1)); ev.append(rng.integers(7, n1, 3 * n1))
+    eu.append(np.arange(0, 6)); ev.append(np.arange(1, 7))
+    # component B: a grid-like ladder, no edge to A
+    b0 = n1
+    nb2 = 5000
+    eu.append(np.arange(b0, b0 + nb2 - 1)); ev.append(np.arange(b0 + 1, b0 + nb2))
+    eu.append(np.arange(b0, b0 + nb2 - 50)); ev.append(np.arange(b0 + 50, b0 + nb2))
+    u = np.concatenate(eu).astype(np.uint32)
+    v = np.concatenate(ev).astype(np.uint32)
+    keep = u != v
+    g = gb.from_edges(n1 + nb2, u[keep], v[keep], False)
+    srcs = np.concatenate([rng.integers(7, n1, 32), rng.integers(b0, b0 + nb2, 32)]).astype(np.uint32)
+    refs = [oracle.bfs_serial(g, int(s)) for s in srcs]
+    for hub_first in (False, True):
+        bfs = gb.GpuBfs(g)
+        if hub_first:
+            bfs.hub_first()
+        for opts in (gb.BfsOptions(force_strategy="bu"), gb.BfsOptions(), gb.BfsOptions(block=512),
+                     gb.BfsOptions(force_strategy="bu", grid_blocks=8)):
+            d = bfs.run_batch(srcs, opts=opts)
+            for i in range(len(srcs)):
+                assert np.array_equal(d[i], refs[i]), (hub_first, i, opts.force_strategy, opts.grid_blocks)
