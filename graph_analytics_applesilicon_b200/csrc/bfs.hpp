@@ -135,6 +135,8 @@ struct gb_bfs {
     void runBatch(const uint32_t* src, int k, const gb_bfs_options& o, std::vector<gb_level>* tr);
     void runPersistentMany(const uint32_t* src, uint32_t count, uint32_t* out, uint64_t stride,
                            const gb_bfs_options& o, float* ms, uint32_t* levels);
+    void runBatchMany(const uint32_t* src, uint32_t count, uint32_t* out, uint64_t stride,
+                      const gb_bfs_options& o, float* ms, uint32_t* levels);
     // Profiling (selector training data).
     size_t profileLevels(uint32_t src, const gb_bfs_options& o, int repeats, float* feats, float* times,
                          size_t cap);

@@ -684,6 +684,88 @@ void gb_bfs::ensureBatch(const gb_bfs_options& o, int k) {
     bGrid = o.grid_blocks > 0 ? std::min<int>((int)o.grid_blocks, bMax) : bMax;
 }
 
+// gb_bfs_run_many for the batched kernel: one launch per group of up to 64
+// sources, then every row of the group returned to the host as the single-
+// source path does (packed to the width the batch's level count allows,
+// copied on the copy stream, widened by host threads) through a ring of
+// kRowRing buffers, so row j + 1's pack and copy overlap row j's widening.
+// The pack kernel checks every depth against the width; a row that does not
+// fit is copied whole.  gpu_ms[i]: the group's launch time shared evenly over
+// its sources; levels[i]: the group's level count.  Without out the last
+// source's depths are left in the handle's depth buffer.
+void gb_bfs::runBatchMany(const uint32_t* src, uint32_t count, uint32_t* out, uint64_t stride,
+                          const gb_bfs_options& o, float* msOut, uint32_t* levelsOut) {
+    constexpr uint32_t kRowRing = 4;
+    static_assert(kRowRing <= kManySlots, "row ring exceeds the handle's pack buffers");
+    validateOptions(o);
+    if (count == 0) return;
+    if (out)
+        for (uint32_t b = 0; b < kRowRing; ++b) {
+            mPackDev[b].ensure(2 * n + 16);
+            mPackHost[b].ensure(2 * n + 16);
+        }
+    mFlag.ensure(kManySlots);
+    mFlagHost.ensure(64);
+    while (mSlotEv.size() < 3 * (size_t)kManySlots + 1 + kMaxInFlight) {
+        cudaEvent_t e;
+        GB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        mSlotEv.push_back(e);
+    }
+    cudaStream_t cs = copyStream.s;
+    for (uint32_t g0 = 0; g0 < count; g0 += 64) {
+        const uint32_t k = std::min<uint32_t>(64, count - g0);
+        runBatch(src + g0, (int)k, o, nullptr);  // returns with the launch finished
+        for (uint32_t j = 0; j < k; ++j) {
+            if (msOut) msOut[g0 + j] = (float)(lastGpuMs / k);
+            if (levelsOut) levelsOut[g0 + j] = lastLevels;
+        }
+        if (!out) {
+            if (g0 + k == count)
+                GB_CUDA(cudaMemcpyAsync(dist.get(), bDist.get() + (uint64_t)(k - 1) * n, n * 4,
+                                        cudaMemcpyDeviceToDevice, stream.s));
+            continue;
+        }
+        const int fmt = packFormat(n, lastLevels);
+        if (fmt < 0) {
+            for (uint32_t j = 0; j < k; ++j)
+                GB_CUDA(cudaMemcpyAsync(out + (uint64_t)(g0 + j) * stride, bDist.get() + (uint64_t)j * n, n * 4,
+                                        cudaMemcpyDeviceToHost, stream.s));
+            GB_CUDA(cudaStreamSynchronize(stream.s));
+            continue;
+        }
+        auto enqueue = [&](uint32_t j) {
+            const uint32_t b = j % kRowRing;
+            cudaEvent_t packed = mSlotEv[b], copied = mSlotEv[kManySlots + b];
+            GB_CUDA(cudaMemsetAsync(mFlag.get() + b, 0, sizeof(unsigned), stream.s));
+            enqueuePack(fmt, bDist.get() + (uint64_t)j * n, n, mPackDev[b].get(), mFlag.get() + b, stream.s);
+            GB_CUDA(cudaEventRecord(packed, stream.s));
+            GB_CUDA(cudaStreamWaitEvent(cs, packed, 0));
+            GB_CUDA(cudaMemcpyAsync(mPackHost[b].p, mPackDev[b].get(), packedBytes(fmt, n), cudaMemcpyDeviceToHost,
+                                    cs));
+            GB_CUDA(cudaMemcpyAsync(mFlagHost.p + j, mFlag.get() + b, sizeof(unsigned), cudaMemcpyDeviceToHost, cs));
+            GB_CUDA(cudaEventRecord(copied, cs));
+        };
+        // buffer b is packed again only after the host has widened its last
+        // row (the host enqueues row j + kRowRing after widening row j)
+        uint32_t queued = 0;
+        for (; queued < k && queued < kRowRing; ++queued) enqueue(queued);
+        for (uint32_t j = 0; j < k; ++j) {
+            const uint32_t b = j % kRowRing;
+            GB_CUDA(cudaEventSynchronize(mSlotEv[kManySlots + b]));
+            uint32_t* dst = out + (uint64_t)(g0 + j) * stride;
+            if (mFlagHost.p[j] == 0) {
+                widenPacked(fmt, mPackHost[b].p, n, dst);
+            } else {  // a depth did not fit the width: the row is still intact on the device
+                GB_CUDA(cudaMemcpyAsync(dst, bDist.get() + (uint64_t)j * n, n * 4, cudaMemcpyDeviceToHost, cs));
+                GB_CUDA(cudaStreamSynchronize(cs));
+            }
+            if (queued < k) enqueue(queued++);
+        }
+    }
+    GB_CUDA(cudaStreamSynchronize(stream.s));
+    GB_CUDA(cudaStreamSynchronize(cs));
+}
+
 void gb_bfs::runBatch(const uint32_t* src, int k, const gb_bfs_options& o, std::vector<gb_level>* tr) {
     validateOptions(o);
     if (k < 1 || k > 64) throw Error(GB_ERR_ARG, "batched BFS takes 1 to 64 sources");

@@ -311,6 +311,10 @@ int gb_bfs_run_many(gb_bfs* h, int variant, const uint32_t* sources, uint32_t co
             h->runPersistentMany(sources, count, out_host, stride, o, gpu_ms, levels);
             return;
         }
+        if (variant == GB_BFS_BATCH) {
+            h->runBatchMany(sources, count, out_host, stride, o, gpu_ms, levels);
+            return;
+        }
         for (uint32_t i = 0; i < count; ++i) {
             switch (variant) {
                 case GB_BFS_VERTEX: h->runVertex(sources[i], o, nullptr); break;

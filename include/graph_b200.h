@@ -170,7 +170,8 @@ typedef enum {
     GB_BFS_DO = 4,         /* gpu_do:     runDO (host loop, one sync per level), bfs_gpu.mm:326-429 */
     GB_BFS_PERSISTENT = 5, /* gpu_do_persistent: every level in one cooperative launch;
                               also what `hybrid` (bfs_gpu.mm:307-325) maps to */
-    GB_BFS_BATCH = 6       /* the 64-source batched kernel (gb_bfs_run_batch; autotune only) */
+    GB_BFS_BATCH = 6       /* the 64-source batched kernel (gb_bfs_run_batch; gb_bfs_run_many;
+                              autotune) */
 } gb_bfs_variant;
 
 typedef enum { GB_SELECT_RULE = 0, GB_SELECT_LEARNED = 1 } gb_selector;
@@ -253,7 +254,11 @@ int gb_bfs_run(gb_bfs* h, int variant, uint32_t source, uint32_t* out_host,
  * depths; else stride >= n), or NULL (the last source's depths stay on the
  * device, gb_bfs_device_dist, whose pointer may change with this call).
  * gpu_ms, levels (each may be NULL): count entries, device time and level
- * count of each traversal.  Every source is checked before any runs. */
+ * count of each traversal.  Every source is checked before any runs.
+ * For GB_BFS_BATCH the sources run 64 to a launch of the batched kernel and
+ * each row is then packed, copied and widened as above; gpu_ms[i] is the
+ * launch's device time shared evenly over its sources and levels[i] the
+ * launch's level count. */
 int gb_bfs_run_many(gb_bfs* h, int variant, const uint32_t* sources, uint32_t count, uint32_t* out_host,
                     uint64_t stride, const gb_bfs_options* opt, float* gpu_ms, uint32_t* levels);
 /* 64-source batched BFS in one persistent launch (replaces the per-source loop

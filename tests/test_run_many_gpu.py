@@ -164,3 +164,37 @@ def test_run_many_in_flight_limits(gb):
     with pytest.raises(gb.GraphError) as e:
         bfs.run_many("gpu_do_persistent", [0], opts=gb.BfsOptions(in_flight=17))
     assert e.value.status == 1 and "in_flight" in str(e.value)
+
+
+def test_run_many_batched_variant(gb, oracle):
+    """gb_bfs_run_many with the batched kernel: 64 sources to a launch, then
+    every row packed, copied and widened.  70 sources make two launches: the
+    first of power-law sources only (4-bit rows), the second with sources on a
+    300-vertex path (150+ levels: byte rows).  Every row equals the oracle's
+    serial BFS, into separate rows, into one reused buffer (the last source's)
+    and kept on the device."""
+    g, first_path = _rmat_plus_path(gb, 300)
+    og = _og(oracle, g)
+    power = [int(s) for s in gb.pick_sources(g, 100, 3) if s < first_path][:64]
+    assert len(power) == 64
+    srcs = np.array(power + [first_path + 150, first_path, g.n - 1, power[0], power[1], first_path + 7], np.uint32)
+    want = [oracle.bfs_serial(og, int(s)) for s in srcs]
+    bfs = gb.GpuBfs(g).hub_first()
+    for sel in ("rule", "learned"):
+        params = gb.default_selector_params("batch")
+        if sel == "learned":
+            if params is None:
+                continue
+            bfs.set_selector(params, 1)
+        o = gb.BfsOptions(selector=sel)
+        out, ms, lv = bfs.run_many("batch", srcs, opts=o)
+        for i in range(len(srcs)):
+            assert np.array_equal(out[i], want[i]), (sel, i)
+        assert (ms > 0).all()
+        assert lv[0] == lv[63] and lv[64] == lv[69] and lv[64] > lv[0]
+        assert lv[0] >= int(max(w[w != 0xFFFFFFFF].max() for w in want[:64])) + 1
+        one = np.empty(g.n, np.uint32)
+        bfs.run_many("batch", srcs, out=one, stride=0, opts=o)
+        assert np.array_equal(one, want[-1])
+        bfs.run_many("batch", srcs[:5], opts=o, device=True)
+        assert np.array_equal(_device_dist(gb, bfs, g.n), want[4])
