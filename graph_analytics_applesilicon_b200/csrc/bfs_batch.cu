@@ -34,7 +34,7 @@ constexpr uint32_t kTraceCap = 1u << 16;
 #define GB_BATCH_BU_COOP 64
 #endif
 #ifndef GB_BATCH_BU_BLOCK
-#define GB_BATCH_BU_BLOCK 512
+#define GB_BATCH_BU_BLOCK 256
 #endif
 // bottom-up list scans: serial per thread for the first kBatchBuSerial entries,
 // then a rest of kBatchBuCoop entries or more by the warp, kBatchBuBlock or
@@ -42,6 +42,10 @@ constexpr uint32_t kTraceCap = 1u << 16;
 constexpr uint32_t kBatchBuSerial = GB_BATCH_BU_SERIAL;
 constexpr uint32_t kBatchBuCoop = GB_BATCH_BU_COOP;
 constexpr uint32_t kBatchBuBlock = GB_BATCH_BU_BLOCK;
+#ifndef GB_BATCH_BU_UNROLL
+#define GB_BATCH_BU_UNROLL 8
+#endif
+constexpr int kBuUnroll = GB_BATCH_BU_UNROLL;  // entries per thread per cooperative step
 
 struct BCounters {
     unsigned acnt;                 // next active queue entries
@@ -422,8 +426,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                 // are loaded at once with their 4 masks.  What is left of a
                 // list then goes to the whole warp (kBatchBuCoop or more
                 // entries left: the warp takes such lists one after another,
-                // 128 entries per step) or to the whole block (kBatchBuBlock or
-                // more left, 4 NT entries per step); shorter rests finish
+                // 32 kBuUnroll entries per step) or to the whole block (kBatchBuBlock or
+                // more left, kBuUnroll NT entries per step); shorter rests finish
                 // serially.  One long list scanned by one thread would hold its
                 // warp, its block and the level.
                 unsigned long long got = 0;
@@ -452,12 +456,12 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                     while (off < hd) {
                         unsigned long long g = 0;
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
+                        for (int q = 0; q < kBuUnroll; ++q) {
                             const uint32_t j = off + laneId() + 32u * q;
                             if (j < hd) g |= fc[a.col_idx[hs + j]];
                         }
                         g2 |= warpOr64(g);
-                        off += 128;
+                        off += 32u * kBuUnroll;
                         if ((g2 & hn) == hn) break;
                     }
                     if (laneId() == (unsigned)l) {
@@ -488,7 +492,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                             while (off < hd) {
                                 unsigned long long g = 0;
 #pragma unroll
-                                for (int q = 0; q < 4; ++q) {
+                                for (int q = 0; q < kBuUnroll; ++q) {
                                     const uint32_t j = off + tid + (uint32_t)NT * q;
                                     if (j < hd) g |= fc[a.col_idx[hs + j]];
                                 }
@@ -499,7 +503,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                                 }
                                 __syncthreads();
                                 g2 = ((unsigned long long)sm.bor[1] << 32) | sm.bor[0];
-                                off += 4u * NT;
+                                off += (uint32_t)kBuUnroll * NT;
                                 if ((g2 & hn) == hn) break;  // block-uniform: all read bor between barriers
                                 __syncthreads();
                             }

@@ -79,7 +79,7 @@ def test_batch_learned_selector_exact(gb, oracle):
 def test_batch_bottom_up_long_lists_exact(gb, oracle):
     """Bottom-up levels hand what is left of a long list to the whole warp
     (64 or more entries left after the thread's own first 64) or to the whole
-    block (512 or more).  Hubs of 100 to 6,000 neighbours in one component and
+    block (256 or more).  Hubs of 100 to 6,000 neighbours in one component and
     half of the sources in another component keep every hub's missing sources
     missing, so its scan runs to the end of its list; lists that finish early
     and short rests finishing serially are in the same warps.  Every source's
