@@ -93,6 +93,7 @@ struct gb_bfs {
     gb::DevBuf<uint32_t> bActive[2], bCand, bHubV[2];
     gb::DevBuf<unsigned long long> bHubOff[2];
     gb::DevBuf<uint32_t> bDist;          // k * n results
+    gb::DevBuf<uint2> bDefer;            // bottom-up: lists whose rest a whole block scans
     int bGrid = 0, bBlock = 0, bMax = 0;
 
     // learned selector parameters (single-source, batched)

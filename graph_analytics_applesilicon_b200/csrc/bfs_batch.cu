@@ -58,6 +58,7 @@ struct BCounters {
     unsigned long long fullEdges;  // degree sum of vertices that became fully seen
     unsigned long long fullCount;
     unsigned long long examined;
+    unsigned dcnt;                 // bottom-up: lists whose rest is deferred to a whole block
 };
 
 struct BArgs {
@@ -73,6 +74,7 @@ struct BArgs {
     uint32_t* hs[2];
     unsigned long long* ho[2];
     uint32_t* cq;
+    uint2* dq;  // bottom-up: (vertex, resume position) of the deferred rests
     uint32_t* dist;
     const uint32_t* sources;
     BCounters* ctr;
@@ -117,10 +119,8 @@ struct BSmem {
     int strat;
     uint32_t base;
     int ok;
-    uint32_t hmask[NT / 32];  // bottom-up: lanes whose list the whole block scans
-    unsigned bor[2];          // OR of the frontier masks found so far (lo, hi)
-    uint32_t hst, hd;
-    unsigned long long hneed;
+    unsigned bor[2];  // bottom-up deferred rests: OR of the frontier masks found (lo, hi)
+    uint32_t dn;      // ... and their count
 };
 
 // Grid barrier after which every thread of the block sees counters *c in
@@ -182,6 +182,29 @@ __device__ __forceinline__ void appendActive(const BArgs& a, BSmem<NT>& sm, bool
         a.ho[nq][i] = old & kHubMask;
     }
     __syncthreads();
+}
+
+// Warp-aggregated form of appendActive (every lane of the warp calls it): no
+// block barrier, so the warps of a block need not wait for one another.
+__device__ __forceinline__ void warpAppendActive(const BArgs& a, bool want, uint32_t v, uint32_t st, uint32_t d,
+                                                 uint32_t nq, BCounters* cur) {
+    const bool hub = want && d >= a.hubMin;
+    const bool q = want && !hub;
+    if (__any_sync(kFull, q)) {
+        const uint32_t p = warpAppend(q, &cur->acnt);
+        if (q) {
+            a.qv[nq][p] = v;
+            a.qs[nq][p] = st;
+            a.qd[nq][p] = d;
+        }
+    }
+    if (hub) {
+        const unsigned long long old = atomicAdd(&cur->hubPack, (1ull << kHubShift) | d);
+        const uint32_t i = (uint32_t)(old >> kHubShift);
+        a.hv[nq][i] = v;
+        a.hs[nq][i] = st;
+        a.ho[nq][i] = old & kHubMask;
+    }
 }
 
 // Fold new bits b into v (owner thread only): seen, next frontier, depths
@@ -426,10 +449,11 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                 // are loaded at once with their 4 masks.  What is left of a
                 // list then goes to the whole warp (kBatchBuCoop or more
                 // entries left: the warp takes such lists one after another,
-                // 32 kBuUnroll entries per step) or to the whole block (kBatchBuBlock or
-                // more left, kBuUnroll NT entries per step); shorter rests finish
+                // 32 kBuUnroll entries per step) or, from kBatchBuBlock entries
+                // left, to a whole block after this loop; shorter rests finish
                 // serially.  One long list scanned by one thread would hold its
-                // warp, its block and the level.
+                // warp and the level; the loop has no block barrier, so the
+                // warps of a block do not wait for one another.
                 unsigned long long got = 0;
                 uint32_t i = st;
                 const uint32_t e = st + d;
@@ -469,53 +493,14 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                         i += min(off, hd);
                     }
                 }
-                {
-                    const unsigned hw = __ballot_sync(kFull, huge);
-                    if (laneId() == 0) sm.hmask[tid >> 5] = hw;
+                // rests of kBatchBuBlock or more entries: deferred to the phase
+                // below (the masks found so far wait in nx, zero in bottom-up levels)
+                if (huge) a.nx[v] = got;
+                if (__any_sync(kFull, huge)) {
+                    const uint32_t p = warpAppend(huge, &cur->dcnt);
+                    if (huge) a.dq[p] = make_uint2((uint32_t)v, i);
                 }
-                if (__syncthreads_or(huge)) {
-                    for (int w = 0; w < NT / 32; ++w) {
-                        for (unsigned hm = sm.hmask[w]; hm; hm &= hm - 1) {
-                            const unsigned owner = (unsigned)w * 32u + (unsigned)(__ffs(hm) - 1);
-                            if (tid == owner) {
-                                sm.hst = i;
-                                sm.hd = e - i;
-                                sm.hneed = want;
-                                sm.bor[0] = 0;
-                                sm.bor[1] = 0;
-                            }
-                            __syncthreads();
-                            const uint32_t hs = sm.hst, hd = sm.hd;
-                            const unsigned long long hn = sm.hneed;
-                            unsigned long long g2 = 0;
-                            uint32_t off = 0;
-                            while (off < hd) {
-                                unsigned long long g = 0;
-#pragma unroll
-                                for (int q = 0; q < kBuUnroll; ++q) {
-                                    const uint32_t j = off + tid + (uint32_t)NT * q;
-                                    if (j < hd) g |= fc[a.col_idx[hs + j]];
-                                }
-                                g = warpOr64(g);
-                                if (laneId() == 0 && g) {
-                                    atomicOr(&sm.bor[0], (unsigned)g);
-                                    atomicOr(&sm.bor[1], (unsigned)(g >> 32));
-                                }
-                                __syncthreads();
-                                g2 = ((unsigned long long)sm.bor[1] << 32) | sm.bor[0];
-                                off += (uint32_t)kBuUnroll * NT;
-                                if ((g2 & hn) == hn) break;  // block-uniform: all read bor between barriers
-                                __syncthreads();
-                            }
-                            if (tid == owner) {
-                                got |= g2;
-                                i += min(off, hd);
-                            }
-                            __syncthreads();
-                        }
-                    }
-                }
-                if (v < a.n) {
+                if (v < a.n && !huge) {
                     if (need) {
                         acc.exam += i - st;
                         b = got & need;
@@ -524,7 +509,75 @@ __global__ void __launch_bounds__(NT, 1024 / NT) batchBfsKernel(BArgs a) {
                     if (b) foldBits(a, v, old, b, d, acc);
                 }
                 writeDepths(a, v, b, level + 1);
-                appendActive<NT>(a, sm, b != 0, (uint32_t)v, st, d, nq, cur);
+                warpAppendActive(a, b != 0, (uint32_t)v, st, d, nq, cur);
+            }
+            // the deferred rests, one at a time per block, taken by ticket over
+            // the whole grid (kBuUnroll NT entries per step, the block's OR of
+            // masks in shared memory, stopping once every missing source is found)
+            if (!batchBarrier<NT>(a, sm, cur)) return;
+            if (tid == 0) sm.dn = ldv32(&cur->dcnt);
+            __syncthreads();
+            const uint32_t D = sm.dn;
+            for (bool first = true;; first = false) {
+                if (tid == 0) sm.item = first ? blockIdx.x : gridDim.x + atomicAdd(&cur->work[0], 1u);
+                __syncthreads();
+                const uint32_t item = sm.item;
+                if (item >= D) break;  // block-uniform
+                const uint2 ent = a.dq[item];
+                const uint32_t v = ent.x, st = a.row_ptr[v], e = a.row_ptr[v + 1];
+                const unsigned long long old = a.seen[v], need = a.all & ~old, got0 = a.nx[v];
+                const unsigned long long hn = need & ~got0;
+                if (tid == 0) {
+                    sm.bor[0] = 0;
+                    sm.bor[1] = 0;
+                }
+                __syncthreads();
+                const uint32_t hd = e - ent.y;
+                unsigned long long g2 = 0;
+                uint32_t off = 0;
+                while (off < hd) {
+                    unsigned long long g = 0;
+#pragma unroll
+                    for (int q = 0; q < kBuUnroll; ++q) {
+                        const uint32_t j = off + tid + (uint32_t)NT * q;
+                        if (j < hd) g |= fc[a.col_idx[ent.y + j]];
+                    }
+                    g = warpOr64(g);
+                    if (laneId() == 0 && g) {
+                        atomicOr(&sm.bor[0], (unsigned)g);
+                        atomicOr(&sm.bor[1], (unsigned)(g >> 32));
+                    }
+                    __syncthreads();
+                    g2 = ((unsigned long long)sm.bor[1] << 32) | sm.bor[0];
+                    off += (uint32_t)kBuUnroll * NT;
+                    if ((g2 & hn) == hn) break;  // block-uniform: all read bor between barriers
+                    __syncthreads();
+                }
+                if (tid == 0) {
+                    const unsigned long long b = (got0 | g2) & need;
+                    const uint32_t d = e - st;
+                    acc.exam += (ent.y - st) + min(off, hd);
+                    a.nx[v] = 0;
+                    a.fr[nq][v] = b;
+                    if (b) {
+                        foldBits(a, v, old, b, d, acc);
+                        for (unsigned long long bb = b; bb; bb &= bb - 1)
+                            a.dist[(uint64_t)(__ffsll((long long)bb) - 1) * a.n + v] = level + 1;
+                        if (d >= a.hubMin) {
+                            const unsigned long long hp = atomicAdd(&cur->hubPack, (1ull << kHubShift) | d);
+                            const uint32_t hi = (uint32_t)(hp >> kHubShift);
+                            a.hv[nq][hi] = v;
+                            a.hs[nq][hi] = st;
+                            a.ho[nq][hi] = hp & kHubMask;
+                        } else {
+                            const uint32_t p = atomicAdd(&cur->acnt, 1u);
+                            a.qv[nq][p] = v;
+                            a.qs[nq][p] = st;
+                            a.qd[nq][p] = d;
+                        }
+                    }
+                }
+                __syncthreads();  // sm.bor and sm.item are reused by the next list
             }
         } else {
             // phase A: clear the previous level's frontier entries of fr[nq]
@@ -672,6 +725,7 @@ void gb_bfs::ensureBatch(const gb_bfs_options& o, int k) {
         bHubOff[i].ensure(hubCap);
     }
     bCand.ensure(n);
+    bDefer.ensure(n);
     bDist.ensure((uint64_t)k * n + 4);
     pctl.ensure(4);
     ptrace.ensure(kTraceCap);
@@ -801,6 +855,7 @@ void gb_bfs::runBatch(const uint32_t* src, int k, const gb_bfs_options& o, std::
         a.ho[i] = bHubOff[i].get();
     }
     a.cq = bCand.get();
+    a.dq = bDefer.get();
     a.dist = bDist.get();
     a.sources = dsrc.get();
     a.ctr = ctr.get();
