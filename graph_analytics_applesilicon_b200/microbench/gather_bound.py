@@ -12,7 +12,7 @@ that flushes L2.  Run from the repository root on a machine with a GPU:
 
 The shared library is compiled on first use next to this file with
     nvcc -shared -Xcompiler -fPIC -gencode arch=compute_100a,code=sm_100a -O3 \
-        -o gather_bound.so gather_bound.cu
+        -o libgather_bound.so gather_bound.cu
 """
 import ctypes as C
 import os
@@ -28,7 +28,7 @@ import graph_analytics_applesilicon_b200 as G  # noqa: E402
 
 
 def load_probe():
-    so = os.path.join(HERE, "gather_bound.so")
+    so = os.path.join(HERE, "libgather_bound.so")
     src = os.path.join(HERE, "gather_bound.cu")
     if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
         subprocess.run(["nvcc", "-shared", "-Xcompiler", "-fPIC", "-gencode", "arch=compute_100a,code=sm_100a",
