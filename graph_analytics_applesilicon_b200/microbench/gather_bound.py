@@ -4,7 +4,8 @@
 Times, on cuda:0, the kernels of gather_bound.cu over the graph's in-lists in the
 degree-adaptive pull's order (vertices by descending in-degree, each list
 sorted) and in the generator's order, beside the library's own gpu_pull_adaptive
-(autotuned, as the benchmark runs it) and gpu_pull_blocked.  Every figure is the
+(autotuned, as the benchmark runs it) and gpu_pull_blocked, then under four vertex
+orderings (in-degree, RCM and their mixes).  Every figure is the
 minimum over repeats of CUDA-event time, each run after a 256 MB buffer write
 that flushes L2.  Run from the repository root on a machine with a GPU:
 
@@ -102,6 +103,30 @@ def main():
     short = 2 * sms * 1024 * 256 // 4
     t = run(2, col_sorted, words=short)
     print(f"{'uniform random ids, 256 per thread (short)':48s} {t:.4f} ms = {4 * short / t / 1e6:7.1f} G gathers/s")
+    del col_sorted, col_gen
+
+    # vertex orderings: does any recover locality beyond the degree skew?
+    rp = torch.from_numpy(g.row_ptr.astype(np.int64)).to(dev)
+    ci = torch.from_numpy(g.col_idx.astype(np.int64)).to(dev)
+    deg = rp[1:] - rp[:-1]
+    rows = torch.repeat_interleave(torch.arange(n, device=dev), deg)
+    rcm = torch.from_numpy(G.reorder_gpu(g, "rcm").astype(np.int64)).to(dev)  # perm[old] = new
+
+    def rank_of(keys):
+        order = torch.sort(keys, stable=True).indices
+        p = torch.empty_like(order)
+        p[order] = torch.arange(n, device=dev)
+        return p
+
+    cls = torch.clamp(torch.floor(torch.log2(deg.clamp(min=1).double())).long(), 0, 30)
+    for label, p in (("in-degree descending", rank_of(-deg)), ("rcm", rcm),
+                     ("in-degree descending, rcm within", rank_of(-deg * (1 << 23) + rcm)),
+                     ("power-of-two classes, rcm within", rank_of((30 - cls) * (1 << 23) + rcm))):
+        col = (torch.sort((p[rows] << 32) | p[ci]).values & 0xFFFFFFFF).to(torch.int32).contiguous()
+        t0, t1 = run(0, col), run(1, col, h=32768, blocks=sms)
+        print(f"order {label:36s} ideal {4 * nvec / t0 / 1e6:6.1f} G/s, ids < 32768 in shared memory "
+              f"{4 * nvec / t1 / 1e6:6.1f} G/s")
+        del col
 
 
 if __name__ == "__main__":
