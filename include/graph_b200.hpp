@@ -266,7 +266,8 @@ public:
         if (tr) tr->assign(buf.begin(), buf.begin() + (long)nl);
     }
     // One traversal per source in one call (the persistent variant queues them
-    // back to back and overlaps each result's copy with the next traversal);
+    // back to back and overlaps each result's copy with the next traversal;
+    // GB_BFS_BATCH runs them 64 to a launch of the batched kernel);
     // out: sources.size() * stride depths (stride 0: one n-entry buffer that
     // ends with the last source's), or null to keep the last result on the device.
     void runMany(int variant, const std::vector<uint32_t>& sources, uint32_t* out, uint64_t stride,
